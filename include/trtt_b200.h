@@ -1,0 +1,215 @@
+/*
+ * trtt_b200.h -- C ABI of libtrtt_b200, the B200 (sm_100a) implementation of
+ * the TRTT forward/back projector pair.
+ *
+ * Two layers:
+ *
+ * 1. Drop-in layer.  Exactly the symbols, signatures, argument meanings and
+ *    return codes of the reference TRTT plugins, so the codger-generated
+ *    Yorick wrappers (plugin/ywrap.c, tomography-LongFessler-model/ywrap.c)
+ *    link against this library unchanged.  Arrays are host double* in the
+ *    reference layouts; every projector ACCUMULATES into `out` (the caller
+ *    zeroes it), except the Long-Fessler routines whose `clr` flag clears the
+ *    destination first, as in the reference.  Return value 0 = TRTT_SUCCESS,
+ *    -1 = TRTT_FAILURE (plugin/trtt_common.h:131,140).  Each call copies its
+ *    inputs to the GPU, computes in FP32 there, and adds the result into
+ *    `out` before returning (synchronous, like the reference).  On failure
+ *    `out` is left unchanged and trtt_b200_last_error() says why.
+ *
+ * 2. Native layer (prefix trtt_b200_).  Device pointers, FP32 data, many
+ *    views per launch, caller-supplied CUDA stream; this is the performance
+ *    path (a plan holds the per-view geometry on the device).
+ *
+ * There is no CPU fallback: without a usable CUDA device every entry point
+ * returns -1.
+ */
+#ifndef TRTT_B200_H
+#define TRTT_B200_H 1
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in layer (reference interfaces)                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces trtt_mvmult, plugin/trtt_common.h:267 (plugin/trtt_common.c:62-69):
+ * out[i[k]-1] += a[k] * in[j[k]-1] for k < number (1-based COO). */
+int trtt_mvmult(double *out, double *in, long number, double *a, long *i, long *j);
+
+/* Replace plugin/trtt_2D_projectors.h:72-82 (plugin/trtt_2D_projectors.c:186-536,
+ * plugin/trtt_2D_projectors_cubic.c:209-398). job 0 = direct (out: nv cells),
+ * job != 0 = transpose (out: nx*ny pixels). */
+int trtt_PB2D(double *out, double *in, long nx, long ny, double s_scl, int s_deg,
+              double *footprint, double *cum_footprint, long size_footprint,
+              double step_footprint, double *coord_footprint, long nv,
+              double v_scl, double *xos, double *xsd, int job);
+int trtt_FB2D(double *out, double *in, long nx, long ny, double s_scl, int s_deg,
+              double *footprint, double *cum_footprint, long size_footprint,
+              double step_footprint, double *coord_footprint, long nv,
+              double v_scl, double *xos, double *xsd, int job);
+int trtt_PB2D_cubic(double *out, double *in, long nx, long ny, double s_scl,
+                    int s_deg, long nv, double v_scl, double *xos, double *xsd,
+                    int job);
+int trtt_FB2D_cubic(double *out, double *in, long nx, long ny, double s_scl,
+                    int s_deg, long nv, double v_scl, double *xos, double *xsd,
+                    int job);
+/* Column (i,j) of the 2D system matrix: out[nv] += H(:, i + j*nx)
+ * (plugin/trtt_2D_projectors.c:393-536). */
+int trtt_PB2D_sparser(double *out, long i, long j, long nx, long ny, double s_scl,
+                      int s_deg, double *footprint, double *cum_footprint,
+                      long size_footprint, double step_footprint,
+                      double *coord_footprint, long nv, double v_scl,
+                      double *xos, double *xsd);
+int trtt_FB2D_sparser(double *out, long i, long j, long nx, long ny, double s_scl,
+                      int s_deg, double *footprint, double *cum_footprint,
+                      long size_footprint, double step_footprint,
+                      double *coord_footprint, long nv, double v_scl,
+                      double *xos, double *xsd);
+
+/* Replace plugin/trtt_3D_projectors.h:299,359,423 and
+ * plugin/trtt_3D_projectors_cubic.h:299,363 (plugin/trtt_3D_projectors.c:959-1338,
+ * plugin/trtt_3D_projectors_cubic.c:506-778).  Volume in[/out] is
+ * [k][j][i] (nx fastest), detector [v][u] (nu fastest). */
+int trtt_PB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+              int s_deg, double *footprint, double *cum_footprint,
+              long size_footprint, double step_footprint, double *coord_footprint,
+              long nu, long nv, double u_scl, double v_scl, double *xos,
+              double *xsd, int job);
+int trtt_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+              int s_deg, double *footprint, double *cum_footprint,
+              long size_footprint, double step_footprint, double *coord_footprint,
+              long nu, long nv, double u_scl, double v_scl, double *xos,
+              double *xsd, int job);
+int trtt_DD_PB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+                 long nu, long nv, double u_scl, double v_scl, double *xos,
+                 double *xsd, int job);
+int trtt_PB3D_cubic(double *out, double *in, long nx, long ny, long nz,
+                    double s_scl, int s_deg, long nu, long nv, double u_scl,
+                    double v_scl, double *xos, double *xsd, int job);
+int trtt_CB3D_cubic(double *out, double *in, long nx, long ny, long nz,
+                    double s_scl, int s_deg, long nu, long nv, double u_scl,
+                    double v_scl, double *xos, double *xsd, int job);
+
+/* Long-Fessler separable-footprint fan-beam model.  The parameter block has
+ * the layout of struct _lf2d_parameters
+ * (tomography-LongFessler-model/LongFessler2D.h:16-28). */
+typedef struct {
+  double pixelSize;
+  double pixelStep;
+  double voxelSize;
+  double sourceDistance;
+  double detectorDistance;
+  double objectOffset1, objectOffset2;
+  long objectDimension1, objectDimension2;
+  long detectorDimension;
+} trtt_b200_lf2d_parameters;
+
+/* Replace tomography-LongFessler-model/LongFessler2D.h:30-70 and the
+ * sparsers declared in tomography-LongFessler-model/ywrap.c:57-77
+ * (LongFessler2D.c:41-681).  void return, as in the reference; a failure
+ * is reported by trtt_b200_last_error() and leaves the destination
+ * unchanged. */
+void lf2d_direct(const void *p, double beta, double detectorOffset,
+                 const double voxel[], double pixel[], int clr);
+void lf2d_line_integ_direct(const void *p, double beta, double detectorOffset,
+                            const double voxel[], double pixel[], int clr);
+void lf2d_adjoint(const void *p, double beta, double detectorOffset,
+                  const double pixel[], double voxel[], int clr);
+void lf2d_line_integ_adjoint(const void *p, double beta, double detectorOffset,
+                             const double pixel[], double voxel[], int clr);
+void lf2d_sparser(const void *p, double beta, double detectorOffset, long i1,
+                  long i2, double pixel[], int clr);
+void lf2d_line_integ_sparser(const void *p, double beta, double detectorOffset,
+                             long i1, long i2, double pixel[], int clr);
+
+/* ------------------------------------------------------------------------ */
+/* Native layer                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Geometry codes (Ytrtt_common.i:70-77). */
+#define TRTT_B200_PARALLEL_BEAM 3
+#define TRTT_B200_CONE_BEAM 4
+#define TRTT_B200_FAN_BEAM 5
+
+/* Volume layouts accepted by the native 3D calls. */
+#define TRTT_B200_LAYOUT_XYZ 0     /* [k][j][i], x fastest (reference) */
+#define TRTT_B200_LAYOUT_COLUMNS 1 /* [j][i][k], z fastest (kernel order) */
+
+/* Message describing the last failure of the calling thread ("" if none). */
+const char *trtt_b200_last_error(void);
+
+/* Library version string. */
+const char *trtt_b200_version(void);
+
+/* Number of kernel launches issued by this process so far (all entry
+ * points, all devices). */
+long trtt_b200_launch_count(void);
+
+typedef struct trtt_b200_plan3d trtt_b200_plan3d;
+
+/* Create a plan for `nviews` views of a 3D parallel or cone beam projector.
+ * cum_footprint == NULL selects the closed-form cubic footprint
+ * (trtt_*3D_cubic); otherwise the table footprint (trtt_*3D) with the given
+ * table (copied).  xos/xsd are nviews*12 coefficients (host).  The plan
+ * copies everything it needs to the current device. */
+int trtt_b200_plan3d_create(trtt_b200_plan3d **plan, int geometry, long nx,
+                            long ny, long nz, double s_scl, int s_deg,
+                            const double *cum_footprint, long size_footprint,
+                            double step_footprint, const double *coord_footprint,
+                            long nu, long nv, double u_scl, double v_scl,
+                            long nviews, const double *xos, const double *xsd);
+
+/* 4D per-gate projection: view k projects the linear temporal interpolation
+ * of gates floor(t_index[k]) and ceil(t_index[k]) (mod nt) with weights
+ * 1-pe, pe (Ytrtt_3D_projectors.i:301-311); the transpose distributes with
+ * the same weights, keeping the reference's handling of an integer
+ * t_index (both indices equal: the later, zero-weight write wins,
+ * Ytrtt_3D_projectors.i:369-371). */
+int trtt_b200_plan3d_set_gates(trtt_b200_plan3d *plan, long nt,
+                               const double *t_index);
+
+/* sino[view-view0][nv][nu] += H_view vol for view in [view0, view0+nview).
+ * vol holds nt volumes (nt = 1 unless gates were set) in `layout`. */
+int trtt_b200_plan3d_forward(trtt_b200_plan3d *plan, const float *vol,
+                             float *sino, long view0, long nview, int layout,
+                             void *stream);
+
+/* vol += sum_view H_view^T sino[view-view0] over [view0, view0+nview). */
+int trtt_b200_plan3d_backward(trtt_b200_plan3d *plan, const float *sino,
+                              float *vol, long view0, long nview, int layout,
+                              void *stream);
+
+/* Synchronise `stream`, then return 0 if no kernel of the plan has flagged
+ * an error since the last call, -1 otherwise (flags are cleared). */
+int trtt_b200_plan3d_status(trtt_b200_plan3d *plan, void *stream);
+
+/* Override the direct-projector band kernel shape (detector rows per CTA
+ * and warps per CTA); 0 keeps the current value.  band_rows < 0 forces the
+ * per-voxel kernel. */
+int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps);
+
+/* 1 if every view of the plan uses the column-factorised kernels. */
+int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
+
+int trtt_b200_plan3d_destroy(trtt_b200_plan3d *plan);
+
+/* Batched host-buffer entry point: the whole scan in one call.  Same
+ * conventions as trtt_CB3D/trtt_CB3D_cubic (host double*, accumulate,
+ * reference layouts) for `nviews` views: xos/xsd are nviews*12, the
+ * detector array is [view][nv][nu].  job 0: out(detector) += H in(volume);
+ * job != 0: out(volume) += H^T in(detector). */
+int trtt_b200_cb3d_batch(double *out, const double *in, long nx, long ny,
+                         long nz, double s_scl, int s_deg,
+                         const double *cum_footprint, long size_footprint,
+                         double step_footprint, const double *coord_footprint,
+                         long nu, long nv, double u_scl, double v_scl,
+                         long nviews, const double *xos, const double *xsd,
+                         int geometry, int job);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRTT_B200_H */

@@ -1,0 +1,116 @@
+"""ctypes binding of libtrtt_b200.so (the CUDA library built from csrc/).
+
+The library is loaded from the package directory; if it is missing it is
+built with nvcc.  There is no fallback: if the library cannot be built or
+loaded, or a call reports failure, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtrtt_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_lp = C.POINTER(C.c_long)
+_vp = C.c_void_p
+_L, _D, _I = C.c_long, C.c_double, C.c_int
+
+# Drop-in symbols with the reference signatures (plugin/ywrap.c:231-403,
+# tomography-LongFessler-model/ywrap.c:6-77) and the native layer
+# (include/trtt_b200.h).
+SIGNATURES = {
+    "trtt_mvmult": (_I, [_dp, _dp, _L, _dp, _lp, _lp]),
+    "trtt_PB2D": (_I, [_dp, _dp, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _D, _dp, _dp, _I]),
+    "trtt_FB2D": (_I, [_dp, _dp, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _D, _dp, _dp, _I]),
+    "trtt_PB2D_cubic": (_I, [_dp, _dp, _L, _L, _D, _I, _L, _D, _dp, _dp, _I]),
+    "trtt_FB2D_cubic": (_I, [_dp, _dp, _L, _L, _D, _I, _L, _D, _dp, _dp, _I]),
+    "trtt_PB2D_sparser": (_I, [_dp, _L, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _D, _dp, _dp]),
+    "trtt_FB2D_sparser": (_I, [_dp, _L, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _D, _dp, _dp]),
+    "trtt_PB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_CB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_DD_PB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_PB3D_cubic": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_CB3D_cubic": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I]),
+    "lf2d_direct": (None, [_vp, _D, _D, _dp, _dp, _I]),
+    "lf2d_line_integ_direct": (None, [_vp, _D, _D, _dp, _dp, _I]),
+    "lf2d_adjoint": (None, [_vp, _D, _D, _dp, _dp, _I]),
+    "lf2d_line_integ_adjoint": (None, [_vp, _D, _D, _dp, _dp, _I]),
+    "lf2d_sparser": (None, [_vp, _D, _D, _L, _L, _dp, _I]),
+    "lf2d_line_integ_sparser": (None, [_vp, _D, _D, _L, _L, _dp, _I]),
+    "trtt_b200_last_error": (C.c_char_p, []),
+    "trtt_b200_version": (C.c_char_p, []),
+    "trtt_b200_launch_count": (_L, []),
+    "trtt_b200_plan3d_create": (_I, [C.POINTER(_vp), _I, _L, _L, _L, _D, _I, _dp, _L, _D, _dp,
+                                      _L, _L, _D, _D, _L, _dp, _dp]),
+    "trtt_b200_plan3d_set_gates": (_I, [_vp, _L, _dp]),
+    "trtt_b200_plan3d_forward": (_I, [_vp, _vp, _vp, _L, _L, _I, _vp]),
+    "trtt_b200_plan3d_backward": (_I, [_vp, _vp, _vp, _L, _L, _I, _vp]),
+    "trtt_b200_plan3d_status": (_I, [_vp, _vp]),
+    "trtt_b200_plan3d_set_tiles": (_I, [_vp, _I, _I]),
+    "trtt_b200_plan3d_factorized": (_I, [_vp]),
+    "trtt_b200_plan3d_destroy": (_I, [_vp]),
+    "trtt_b200_cb3d_batch": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
+                                   _D, _L, _dp, _dp, _I, _I]),
+}
+
+
+class TrttError(RuntimeError):
+    """A libtrtt_b200 call reported failure (TRTT_FAILURE)."""
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load (building if needed) libtrtt_b200.so and bind its symbols."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH) and build_if_missing:
+            from . import build as _build
+            _build.build()
+        if not os.path.exists(LIB_PATH):
+            raise TrttError(f"libtrtt_b200.so not found at {LIB_PATH}")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    msg = load().trtt_b200_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise TrttError(f"{what} failed: {last_error()}")
+
+
+def launch_count() -> int:
+    return int(load().trtt_b200_launch_count())
+
+
+def dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)
+
+
+def lptr(a: np.ndarray):
+    if a.dtype != np.int64 or not a.flags.c_contiguous:
+        raise TypeError("expected a C-contiguous int64 array")
+    return a.ctypes.data_as(_lp)

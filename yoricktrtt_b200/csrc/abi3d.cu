@@ -1,0 +1,559 @@
+// abi3d.cu -- C ABI of the 3D projectors: the drop-in trtt_PB3D/CB3D(_cubic)
+// symbols, the batched host-buffer entry point and the native plan API.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "runtime.h"
+#include "../../include/trtt_b200.h"
+
+using namespace trtt;
+
+namespace {
+
+// Per-view constants of the 3D projectors, derived in FP64 with the operand
+// order of the reference so that the device sees the reference's values
+// (cone beam plugin/trtt_3D_projectors.c:1186-1230, parallel beam
+// plugin/trtt_3D_projectors.c:963-1004; identical in the _cubic file).
+void make_view3d(const Params3D &P, const double *xos, const double *xsd, View3D &V)
+{
+  std::memset(&V, 0, sizeof(V));
+  const double a1 = xsd[0], a2 = xsd[1], a3 = xsd[2], a4 = xsd[3];
+  const double a5 = xsd[4], a6 = xsd[5], a7 = xsd[6], a8 = xsd[7];
+  const double a9 = xsd[8], a10 = xsd[9], a11 = xsd[10], a12 = xsd[11];
+  const double o1 = xos[0], o2 = xos[1], o3 = xos[2], o4 = xos[3];
+  const double o5 = xos[4], o6 = xos[5], o7 = xos[6], o8 = xos[7];
+  const double o9 = xos[8], o10 = xos[9], o11 = xos[10], o12 = xos[11];
+  const double a1inv = -1.0 * (1.0 / a1);
+  const double b1 = a6 + a1inv * a5 * a2, c1 = a10 + a1inv * a9 * a2;
+  const double b2 = a7 + a1inv * a5 * a3, c2 = a11 + a1inv * a9 * a3;
+  const double b3 = a8 + a1inv * a5 * a4, c3 = a12 + a1inv * a9 * a4;
+  V.o1 = o1; V.o2 = o2; V.o3 = o3; V.o4 = o4;
+  V.nv_x = b1 * o5 + b2 * o9;  V.nu_x = c1 * o5 + c2 * o9;
+  V.nv_y = b1 * o6 + b2 * o10; V.nu_y = c1 * o6 + c2 * o10;
+  V.nv_z = b1 * o7 + b2 * o11; V.nu_z = c1 * o7 + c2 * o11;
+  V.nv_c = b1 * o8 + b2 * o12; V.nu_c = c1 * o8 + c2 * o12;
+  V.d_x = a1 * o1 + a2 * o5 + a3 * o9;
+  V.d_y = a1 * o2 + a2 * o6 + a3 * o10;
+  V.d_z = a1 * o3 + a2 * o7 + a3 * o11;
+  V.d_c = a1 * o4 + a2 * o8 + a3 * o12;
+  V.a4sqr = a4 * a4;
+  V.a4m = -1.0 * a4;
+  V.a8 = a8;
+  V.a12 = a12;
+  V.b3 = b3;
+  V.c3 = c3;
+  // parallel beam
+  V.v_x = b1 * o5 + b2 * o9;  V.u_x = c1 * o5 + c2 * o9;
+  V.v_y = b1 * o6 + b2 * o10; V.u_y = c1 * o6 + c2 * o10;
+  V.v_z = b1 * o7 + b2 * o11; V.u_z = c1 * o7 + c2 * o11;
+  V.v_c = b1 * o8 + b2 * o12 + b3; V.u_c = c1 * o8 + c2 * o12 + c3;
+  const double a1sqr = a1 * a1;
+  const double a5sqr = P.v_scl * P.v_scl * a5 * a5;
+  const double a9sqr = P.u_scl * P.u_scl * a9 * a9;
+  const double delta_u = std::sqrt(1.0 + (a9sqr / (a1sqr + a5sqr)));
+  const double delta_v = std::sqrt(1.0 + (a5sqr / a1sqr));
+  V.p_rho0 = P.s_scl * P.s_scl * P.s_scl * delta_u * delta_v;
+  V.p_h_u = P.s_scl / P.u_scl;
+  V.p_h_v = P.s_scl / P.v_scl;
+  V.p_scl_u = 1.0 / V.p_h_u;
+  V.p_scl_v = 1.0 / V.p_h_v;
+  V.p_hs_u = P.hs0 * V.p_h_u;
+  V.p_hs_v = P.hs0 * V.p_h_v;
+  V.p_sclt_u = V.p_scl_u / P.step;
+  V.p_sclt_v = V.p_scl_v / P.step;
+  V.g0 = 0;
+  V.g1 = 0;
+  V.w0 = 1.0f;
+  V.w1 = 0.0f;
+  if (P.geom == GEOM_CONE)
+    V.factorized = (V.o3 == 0.0 && V.d_z == 0.0 && V.nv_z == 0.0) ? 1 : 0;
+  else
+    V.factorized = (V.v_z == 0.0) ? 1 : 0;
+}
+
+Params3D make_params(int geom, long nx, long ny, long nz, double s_scl, int s_deg,
+                     const double *cum_dev, long size, double step,
+                     double coord0, long nu, long nv, double u_scl, double v_scl)
+{
+  Params3D P;
+  std::memset(&P, 0, sizeof(P));
+  P.geom = geom;
+  P.model = cum_dev ? MODEL_TABLE : MODEL_CUBIC;
+  P.nx = (int)nx; P.ny = (int)ny; P.nz = (int)nz;
+  P.nu = (int)nu; P.nv = (int)nv;
+  P.nt = 1;
+  P.s_scl = s_scl;
+  P.u_scl = u_scl;
+  P.v_scl = v_scl;
+  P.rho0_init = s_scl * s_scl * s_scl;
+  P.h_u0 = s_scl / u_scl;
+  P.h_v0 = s_scl / v_scl;
+  P.hs0 = 0.5 * (s_deg + 1);
+  P.cum = cum_dev;
+  P.size = (int)size;
+  P.last = (double)(size - 1);
+  P.step = cum_dev ? step : 1.0;
+  P.coord0 = coord0;
+  return P;
+}
+
+// Band shape of the direct kernel for a detector nu cells wide.
+void choose_band(int nu, int nv, int &band_rows, int &warps)
+{
+  const long budget = 200 * 1024;
+  warps = 16;
+  while (warps > 2 && (long)warps * nu * 4 > budget / 3) warps /= 2;
+  const long rest = budget - (long)warps * nu * 4;
+  long rows = rest / ((long)nu * 4 + (long)warps * 4);
+  if (rows > 64) rows = 64;
+  if (rows > nv) rows = nv;
+  band_rows = rows >= 2 ? (int)rows : 0;
+}
+
+int geom_code(int geometry)
+{
+  if (geometry == TRTT_B200_PARALLEL_BEAM) return GEOM_PARALLEL;
+  if (geometry == TRTT_B200_CONE_BEAM || geometry == TRTT_B200_FAN_BEAM) return GEOM_CONE;
+  return -1;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+struct trtt_b200_plan3d {
+  Params3D P;
+  int device = 0;
+  long nviews = 0;
+  int nt = 1;
+  int band_rows = 0, warps = 16;
+  bool factorized = true;
+  DevBuf views, cum, gate_ptr, entries, scratch, err;
+  std::vector<View3D> hviews;
+};
+
+static int upload_gates(trtt_b200_plan3d *pl, const std::vector<std::vector<GateEntry>> &lists)
+{
+  std::vector<int> ptr(lists.size() + 1, 0);
+  std::vector<GateEntry> ent;
+  for (size_t g = 0; g < lists.size(); ++g) {
+    ptr[g] = (int)ent.size();
+    ent.insert(ent.end(), lists[g].begin(), lists[g].end());
+  }
+  ptr[lists.size()] = (int)ent.size();
+  TRTT_CK(pl->gate_ptr.ensure(sizeof(int) * ptr.size()));
+  TRTT_CK(pl->entries.ensure(sizeof(GateEntry) * (ent.empty() ? 1 : ent.size())));
+  TRTT_CK(cudaMemcpy(pl->gate_ptr.p, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
+  if (!ent.empty())
+    TRTT_CK(cudaMemcpy(pl->entries.p, ent.data(), sizeof(GateEntry) * ent.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_create(trtt_b200_plan3d **plan, int geometry,
+                                       long nx, long ny, long nz, double s_scl,
+                                       int s_deg, const double *cum_footprint,
+                                       long size_footprint, double step_footprint,
+                                       const double *coord_footprint, long nu,
+                                       long nv, double u_scl, double v_scl,
+                                       long nviews, const double *xos,
+                                       const double *xsd)
+{
+  clear_error();
+  if (!plan) return fail("plan3d_create: null plan pointer");
+  *plan = nullptr;
+  const int g = geom_code(geometry);
+  if (g < 0) return fail("plan3d_create: geometry must be 3 (parallel), 4 (cone) or 5 (fan)");
+  if (!dim_ok(nx) || !dim_ok(ny) || !dim_ok(nz) || !dim_ok(nu) || !dim_ok(nv) || !dim_ok(nviews))
+    return fail("plan3d_create: sizes must be in [1, 2^30)");
+  if (nx * ny >= (1L << 31) || nx * ny * nz >= (1L << 40))
+    return fail("plan3d_create: volume too large");
+  if (!xos || !xsd) return fail("plan3d_create: null xos/xsd");
+  if (cum_footprint && (size_footprint < 1 || !coord_footprint || !(step_footprint > 0)))
+    return fail("plan3d_create: invalid footprint table");
+  trtt_b200_plan3d *pl = new (std::nothrow) trtt_b200_plan3d();
+  if (!pl) return fail("plan3d_create: out of host memory");
+  cudaGetDevice(&pl->device);
+  if (cum_footprint) {
+    cudaError_t e = pl->cum.ensure(sizeof(double) * size_footprint);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(pl->cum.p, cum_footprint, sizeof(double) * size_footprint, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      delete pl;
+      return fail_cuda(e, "plan3d_create(footprint)");
+    }
+  }
+  pl->P = make_params(g, nx, ny, nz, s_scl, s_deg, cum_footprint ? pl->cum.as<double>() : nullptr,
+                      size_footprint, step_footprint, cum_footprint ? coord_footprint[0] : 0.0,
+                      nu, nv, u_scl, v_scl);
+  pl->nviews = nviews;
+  pl->hviews.resize(nviews);
+  for (long v = 0; v < nviews; ++v) {
+    make_view3d(pl->P, xos + 12 * v, xsd + 12 * v, pl->hviews[v]);
+    if (!pl->hviews[v].factorized) pl->factorized = false;
+  }
+  choose_band(pl->P.nu, pl->P.nv, pl->band_rows, pl->warps);
+  cudaError_t e = pl->views.ensure(sizeof(View3D) * nviews);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(pl->views.p, pl->hviews.data(), sizeof(View3D) * nviews, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = pl->err.ensure(sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(pl->err.p, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    delete pl;
+    return fail_cuda(e, "plan3d_create(upload)");
+  }
+  std::vector<std::vector<GateEntry>> lists(1);
+  for (long v = 0; v < nviews; ++v) lists[0].push_back(GateEntry{(int)v, 1.0f});
+  if (upload_gates(pl, lists)) {
+    delete pl;
+    return -1;
+  }
+  *plan = pl;
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_set_gates(trtt_b200_plan3d *pl, long nt, const double *t_index)
+{
+  clear_error();
+  if (!pl || !t_index) return fail("plan3d_set_gates: null argument");
+  if (nt < 1 || nt > 65535) return fail("plan3d_set_gates: nt must be in [1, 65535]");
+  std::vector<std::vector<GateEntry>> lists(nt);
+  for (long v = 0; v < pl->nviews; ++v) {
+    const double t = t_index[v];
+    if (!(t >= 0.0 && t <= (double)nt))
+      return fail("plan3d_set_gates: t_index must lie in [0, nt] (Ytrtt_3D_projectors.i:289-292)");
+    const double f = std::floor(t), c = std::ceil(t);
+    const double pe = t - f;
+    const int g0 = (int)((long)f % nt), g1 = (int)((long)c % nt);
+    View3D &V = pl->hviews[v];
+    V.g0 = g0;
+    V.g1 = g1;
+    V.w0 = (float)(1.0 - pe);
+    V.w1 = (float)pe;
+    if (g0 != g1) {
+      lists[g0].push_back(GateEntry{(int)v, (float)(1.0 - pe)});
+      lists[g1].push_back(GateEntry{(int)v, (float)pe});
+    } else {
+      // both interpolation indices equal: Yorick's repeated-index
+      // assignment keeps the second (weight pe) write
+      lists[g0].push_back(GateEntry{(int)v, (float)pe});
+      V.w0 = (float)((1.0 - pe) + pe);
+      V.w1 = 0.0f;
+    }
+  }
+  TRTT_CK(cudaMemcpy(pl->views.p, pl->hviews.data(), sizeof(View3D) * pl->nviews, cudaMemcpyHostToDevice));
+  pl->nt = (int)nt;
+  pl->P.nt = (int)nt;
+  return upload_gates(pl, lists);
+}
+
+extern "C" int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *pl, int band_rows, int warps)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_tiles: null plan");
+  if (warps > 0) {
+    if (warps < 2 || warps > 16) return fail("plan3d_set_tiles: warps must be in [2, 16]");
+    pl->warps = warps;
+  }
+  if (band_rows < 0) {
+    pl->band_rows = 0;
+  } else if (band_rows > 0) {
+    const long smem = 4L * ((long)band_rows * pl->P.nu + (long)pl->warps * pl->P.nu + (long)pl->warps * band_rows);
+    if (smem > 227L * 1024) return fail("plan3d_set_tiles: band does not fit in shared memory");
+    pl->band_rows = band_rows > pl->P.nv ? pl->P.nv : band_rows;
+  }
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
+{
+  return pl && pl->factorized ? 1 : 0;
+}
+
+static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long view0,
+                    long nview, int layout, void *stream, bool forward)
+{
+  clear_error();
+  if (!pl || !src || !dst) return fail("plan3d: null argument");
+  if (view0 < 0 || nview < 0 || view0 + nview > pl->nviews) return fail("plan3d: view range out of bounds");
+  if (layout != TRTT_B200_LAYOUT_XYZ && layout != TRTT_B200_LAYOUT_COLUMNS)
+    return fail("plan3d: unknown volume layout");
+  if (nview == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  const Params3D &P = pl->P;
+  const long nvox = (long)P.nx * P.ny * P.nz;
+  const long npix = (long)P.nu * P.nv;
+  const float *volc = forward ? src : nullptr;
+  float *volo = forward ? nullptr : dst;
+  if (layout == TRTT_B200_LAYOUT_XYZ) {
+    TRTT_CK(pl->scratch.ensure(sizeof(float) * nvox * pl->nt));
+    if (forward) {
+      TRTT_CK(xyz_f32_to_col_f32(src, pl->scratch.as<float>(), P.nx, P.ny, P.nz, pl->nt, st));
+      count_launch();
+      volc = pl->scratch.as<float>();
+    } else {
+      TRTT_CK(cudaMemsetAsync(pl->scratch.p, 0, sizeof(float) * nvox * pl->nt, st));
+      volo = pl->scratch.as<float>();
+    }
+  }
+  if (forward) {
+    Fwd3DLaunch L;
+    L.P = P;
+    L.views = pl->views.as<View3D>() + view0;
+    L.nviews = (int)nview;
+    L.vol = volc;
+    L.gate_stride = nvox;
+    L.sino = dst;
+    L.sino_view_stride = npix;
+    L.band_rows = pl->factorized ? pl->band_rows : 0;
+    L.warps = pl->warps;
+    L.err = pl->err.as<int>();
+    TRTT_CK(launch_fwd3d(L, st));
+    count_launch();
+  } else {
+    Back3DLaunch L;
+    L.P = P;
+    L.views = pl->views.as<View3D>();
+    L.gate_ptr = pl->gate_ptr.as<int>();
+    L.entries = pl->entries.as<GateEntry>();
+    L.ngates = pl->nt;
+    L.view_lo = (int)view0;
+    L.view_hi = (int)(view0 + nview);
+    L.sino = src;
+    L.sino_view_stride = npix;
+    L.vol = volo;
+    L.gate_stride = nvox;
+    L.factorized = pl->factorized ? 1 : 0;
+    L.err = pl->err.as<int>();
+    TRTT_CK(launch_back3d(L, st));
+    count_launch();
+    if (layout == TRTT_B200_LAYOUT_XYZ) {
+      TRTT_CK(col_f32_add_to_xyz_f32(volo, dst, P.nx, P.ny, P.nz, pl->nt, st));
+      count_launch();
+    }
+  }
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_forward(trtt_b200_plan3d *pl, const float *vol, float *sino,
+                                        long view0, long nview, int layout, void *stream)
+{
+  return plan_run(pl, vol, sino, view0, nview, layout, stream, true);
+}
+
+extern "C" int trtt_b200_plan3d_backward(trtt_b200_plan3d *pl, const float *sino, float *vol,
+                                         long view0, long nview, int layout, void *stream)
+{
+  return plan_run(pl, sino, vol, view0, nview, layout, stream, false);
+}
+
+extern "C" int trtt_b200_plan3d_status(trtt_b200_plan3d *pl, void *stream)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_status: null plan");
+  int h = 0;
+  TRTT_CK(cudaStreamSynchronize((cudaStream_t)stream));
+  TRTT_CK(cudaMemcpy(&h, pl->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  TRTT_CK(cudaMemset(pl->err.p, 0, sizeof(int)));
+  if (h & TRTT_ERR_SOURCE_PLANE) return fail("a voxel lies in the source plane (wk == 0)");
+  if (h) return fail("device error flag set");
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_destroy(trtt_b200_plan3d *pl)
+{
+  if (!pl) return 0;
+  pl->views.release();
+  pl->cum.release();
+  pl->gate_ptr.release();
+  pl->entries.release();
+  pl->scratch.release();
+  pl->err.release();
+  delete pl;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Host-buffer entry points (drop-in and batched)
+// ---------------------------------------------------------------------------
+namespace {
+
+// One call of a 3D projector on host double* arrays for `nviews` views:
+// out += H in (job 0) or out += H^T in (job != 0), reference layouts.
+int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
+           double s_scl, int s_deg, const double *cum, long size, double step,
+           const double *coord, long nu, long nv, double u_scl, double v_scl,
+           long nviews, const double *xos, const double *xsd, int job)
+{
+  clear_error();
+  if (!out || !in || !xos || !xsd) return fail("null array argument");
+  if (!dim_ok(nx) || !dim_ok(ny) || !dim_ok(nz) || !dim_ok(nu) || !dim_ok(nv) || !dim_ok(nviews))
+    return fail("dimensions must be in [1, 2^30)");
+  if (cum && (size < 1 || !coord)) return fail("invalid footprint table");
+  DropIn &D = dropin();
+  std::lock_guard<std::mutex> lock(D.mu);
+  TRTT_CK(D.init());
+  TRTT_CK(cudaSetDevice(D.device));
+  cudaStream_t st = D.stream;
+  const long nvox = nx * ny * nz;
+  const long npix = nu * nv * nviews;
+  const long nin = job == 0 ? nvox : npix, nout = job == 0 ? npix : nvox;
+  // footprint table
+  const double *cum_dev = nullptr;
+  if (cum) {
+    TRTT_CK(D.aux.ensure(sizeof(double) * size));
+    TRTT_CK(cudaMemcpyAsync(D.aux.p, cum, sizeof(double) * size, cudaMemcpyHostToDevice, st));
+    cum_dev = D.aux.as<double>();
+  }
+  Params3D P = make_params(geom, nx, ny, nz, s_scl, s_deg, cum_dev, size, step,
+                           cum ? coord[0] : 0.0, nu, nv, u_scl, v_scl);
+  std::vector<View3D> hv(nviews);
+  bool fact = true;
+  for (long v = 0; v < nviews; ++v) {
+    make_view3d(P, xos + 12 * v, xsd + 12 * v, hv[v]);
+    fact = fact && hv[v].factorized;
+  }
+  TRTT_CK(D.geom.ensure(sizeof(View3D) * nviews));
+  TRTT_CK(cudaMemcpyAsync(D.geom.p, hv.data(), sizeof(View3D) * nviews, cudaMemcpyHostToDevice, st));
+  TRTT_CK(D.err.ensure(sizeof(int)));
+  TRTT_CK(cudaMemsetAsync(D.err.p, 0, sizeof(int), st));
+  TRTT_CK(D.in64.ensure(sizeof(double) * nin));
+  TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+  TRTT_CK(D.vol32.ensure(sizeof(float) * nvox));
+  TRTT_CK(D.det32.ensure(sizeof(float) * npix));
+  if (job == 0) {
+    TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
+    TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
+    Fwd3DLaunch L;
+    L.P = P;
+    L.views = D.geom.as<View3D>();
+    L.nviews = (int)nviews;
+    L.vol = D.vol32.as<float>();
+    L.gate_stride = nvox;
+    L.sino = D.det32.as<float>();
+    L.sino_view_stride = nu * nv;
+    int rows = 0, warps = 16;
+    choose_band((int)nu, (int)nv, rows, warps);
+    L.band_rows = fact ? rows : 0;
+    L.warps = warps;
+    L.err = D.err.as<int>();
+    TRTT_CK(launch_fwd3d(L, st));
+    count_launch(2);
+  } else {
+    TRTT_CK(f64_to_f32(D.in64.as<double>(), D.det32.as<float>(), npix, st));
+    TRTT_CK(cudaMemsetAsync(D.vol32.p, 0, sizeof(float) * nvox, st));
+    std::vector<int> gp = {0, (int)nviews};
+    std::vector<GateEntry> ge(nviews);
+    for (long v = 0; v < nviews; ++v) ge[v] = GateEntry{(int)v, 1.0f};
+    TRTT_CK(D.gates.ensure(sizeof(int) * 2 + sizeof(GateEntry) * nviews + 16));
+    int *gp_dev = D.gates.as<int>();
+    GateEntry *ge_dev = reinterpret_cast<GateEntry *>(D.gates.as<char>() + 16);
+    TRTT_CK(cudaMemcpyAsync(gp_dev, gp.data(), sizeof(int) * 2, cudaMemcpyHostToDevice, st));
+    TRTT_CK(cudaMemcpyAsync(ge_dev, ge.data(), sizeof(GateEntry) * nviews, cudaMemcpyHostToDevice, st));
+    Back3DLaunch L;
+    L.P = P;
+    L.views = D.geom.as<View3D>();
+    L.gate_ptr = gp_dev;
+    L.entries = ge_dev;
+    L.ngates = 1;
+    L.view_lo = 0;
+    L.view_hi = (int)nviews;
+    L.sino = D.det32.as<float>();
+    L.sino_view_stride = nu * nv;
+    L.vol = D.vol32.as<float>();
+    L.gate_stride = nvox;
+    L.factorized = fact ? 1 : 0;
+    L.err = D.err.as<int>();
+    TRTT_CK(launch_back3d(L, st));
+    count_launch(2);
+  }
+  int herr = 0;
+  TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TRTT_CK(cudaStreamSynchronize(st));
+  if (herr & TRTT_ERR_SOURCE_PLANE) {
+    std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
+    return fail("a voxel lies in the source plane (wk == 0)");
+  }
+  // out += result (FP64 accumulation on the device)
+  TRTT_CK(D.out64.ensure(sizeof(double) * nout));
+  TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, st));
+  if (job == 0) {
+    TRTT_CK(f32_add_to_f64(D.det32.as<float>(), D.out64.as<double>(), npix, st));
+  } else {
+    TRTT_CK(col_f32_add_to_xyz_f64(D.vol32.as<float>(), D.out64.as<double>(), (int)nx, (int)ny, (int)nz, 1, st));
+  }
+  count_launch();
+  TRTT_CK(cudaMemcpyAsync(out, D.out64.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
+  TRTT_CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trtt_PB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+              int s_deg, double *footprint, double *cum_footprint,
+              long size_footprint, double step_footprint, double *coord_footprint,
+              long nu, long nv, double u_scl, double v_scl, double *xos,
+              double *xsd, int job)
+{
+  (void)footprint;
+  if (!cum_footprint) return fail("trtt_PB3D: null cum_footprint");
+  return host3d(GEOM_PARALLEL, out, in, nx, ny, nz, s_scl, s_deg, cum_footprint,
+                size_footprint, step_footprint, coord_footprint, nu, nv, u_scl, v_scl,
+                1, xos, xsd, job);
+}
+
+int trtt_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+              int s_deg, double *footprint, double *cum_footprint,
+              long size_footprint, double step_footprint, double *coord_footprint,
+              long nu, long nv, double u_scl, double v_scl, double *xos,
+              double *xsd, int job)
+{
+  (void)footprint;
+  if (!cum_footprint) return fail("trtt_CB3D: null cum_footprint");
+  return host3d(GEOM_CONE, out, in, nx, ny, nz, s_scl, s_deg, cum_footprint,
+                size_footprint, step_footprint, coord_footprint, nu, nv, u_scl, v_scl,
+                1, xos, xsd, job);
+}
+
+int trtt_PB3D_cubic(double *out, double *in, long nx, long ny, long nz,
+                    double s_scl, int s_deg, long nu, long nv, double u_scl,
+                    double v_scl, double *xos, double *xsd, int job)
+{
+  return host3d(GEOM_PARALLEL, out, in, nx, ny, nz, s_scl, s_deg, nullptr, 0, 1.0,
+                nullptr, nu, nv, u_scl, v_scl, 1, xos, xsd, job);
+}
+
+int trtt_CB3D_cubic(double *out, double *in, long nx, long ny, long nz,
+                    double s_scl, int s_deg, long nu, long nv, double u_scl,
+                    double v_scl, double *xos, double *xsd, int job)
+{
+  return host3d(GEOM_CONE, out, in, nx, ny, nz, s_scl, s_deg, nullptr, 0, 1.0,
+                nullptr, nu, nv, u_scl, v_scl, 1, xos, xsd, job);
+}
+
+int trtt_b200_cb3d_batch(double *out, const double *in, long nx, long ny, long nz,
+                         double s_scl, int s_deg, const double *cum_footprint,
+                         long size_footprint, double step_footprint,
+                         const double *coord_footprint, long nu, long nv,
+                         double u_scl, double v_scl, long nviews,
+                         const double *xos, const double *xsd, int geometry,
+                         int job)
+{
+  const int g = geom_code(geometry);
+  if (g < 0) return fail("cb3d_batch: geometry must be 3, 4 or 5");
+  return host3d(g, out, in, nx, ny, nz, s_scl, s_deg, cum_footprint, size_footprint,
+                step_footprint, coord_footprint, nu, nv, u_scl, v_scl, nviews, xos, xsd,
+                job);
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// kernels.h -- launch descriptors and launcher entry points of the device
+// kernels (internal to libtrtt_b200; the public C ABI is include/trtt_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "trtt_types.h"
+
+namespace trtt {
+
+// Device error bits written by kernels into a flag word.
+enum : int {
+  TRTT_ERR_SOURCE_PLANE = 1,  // a voxel lies in the source plane (wk == 0)
+  TRTT_ERR_BAD_INDEX = 2,     // sparse index out of range
+};
+
+// One (view, weight) contribution to a gate in the transpose.
+struct GateEntry {
+  int view;
+  float w;
+};
+
+struct Fwd3DLaunch {
+  Params3D P;
+  const View3D *views;   // device, nviews entries
+  int nviews;
+  const float *vol;      // column layout [gate][j][i][k]
+  long gate_stride;      // nx*ny*nz
+  float *sino;           // [view][nv][nu], accumulated
+  long sino_view_stride; // nv*nu
+  int band_rows;         // > 0: band kernel (factorised views); 0: per-voxel
+  int warps;             // warps per CTA of the band kernel
+  int *err;              // device error flags
+};
+
+struct Back3DLaunch {
+  Params3D P;
+  const View3D *views;
+  const int *gate_ptr;   // ngates+1 offsets into entries
+  const GateEntry *entries;
+  int ngates;
+  int view_lo, view_hi;  // entries outside [view_lo, view_hi) are skipped
+  const float *sino;     // detector images of views view_lo..view_hi-1
+  long sino_view_stride;
+  float *vol;            // column layout, accumulated
+  long gate_stride;
+  int factorized;        // 1: column kernel; 0: per-voxel kernel
+  int *err;
+};
+
+cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st);
+cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st);
+
+// Layout / precision conversions (convert.cu).
+// XYZ layout is the reference's [k][j][i] (x fastest); column layout is
+// [j][i][k] (k fastest).  `nb` volumes are converted back to back.
+cudaError_t xyz_f64_to_col_f32(const double *src, float *dst, int nx, int ny,
+                               int nz, int nb, cudaStream_t st);
+cudaError_t xyz_f32_to_col_f32(const float *src, float *dst, int nx, int ny,
+                               int nz, int nb, cudaStream_t st);
+cudaError_t col_f32_add_to_xyz_f64(const float *src, double *dst, int nx,
+                                   int ny, int nz, int nb, cudaStream_t st);
+cudaError_t col_f32_add_to_xyz_f32(const float *src, float *dst, int nx,
+                                   int ny, int nz, int nb, cudaStream_t st);
+cudaError_t f64_to_f32(const double *src, float *dst, long n, cudaStream_t st);
+cudaError_t f32_add_to_f64(const float *src, double *dst, long n, cudaStream_t st);
+
+}  // namespace trtt

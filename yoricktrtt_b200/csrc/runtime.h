@@ -1,0 +1,58 @@
+// runtime.h -- host runtime shared by the C ABI translation units: device
+// context, cached device buffers, error reporting, launch accounting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+namespace trtt {
+
+// Thread-local last-error message.
+void set_error(const std::string &msg);
+void clear_error();
+
+// Count of kernel launches issued by the library.
+extern std::atomic<long> g_launches;
+inline void count_launch(long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Growable device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need);
+  void release();
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Process-wide state of the drop-in (host-buffer) entry points: one device,
+// one stream, scratch buffers reused across calls, serialised by a mutex
+// (the reference plugin is single-threaded and synchronous).
+struct DropIn {
+  std::mutex mu;
+  bool ready = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf in64, out64, vol32, det32, geom, gates, aux, err;
+  cudaError_t init();
+};
+DropIn &dropin();
+
+// Report a CUDA error and return -1 (for use in `return fail_cuda(...)`).
+int fail_cuda(cudaError_t e, const char *what);
+int fail(const std::string &msg);
+
+// Check that a long dimension is positive and fits the kernels' int indices.
+bool dim_ok(long n);
+
+}  // namespace trtt
+
+#define TRTT_CK(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return trtt::fail_cuda(e_, #call); \
+  } while (0)

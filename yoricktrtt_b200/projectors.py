@@ -1,0 +1,183 @@
+"""Operator layer: multi-view B200 projectors on device-resident tensors.
+
+Mirrors the Yorick operator layer of TRTT (``Ytrtt_3D_projectors.i:56-187``):
+a projector is built from a tomographic object and a set of views and is
+applied as ``C(x, job)`` with ``job`` 0 = direct and 1 = transpose.  Here one
+``Projector3D`` holds all views of a scan on the GPU (a ``trtt_b200_plan3d``)
+and applies them in a single launch per direction; ``single_view`` returns
+the per-view closure of the reference (``A_single_3D``).
+
+Tensors are torch CUDA float32.  Volumes are (nz, ny, nx) in the reference
+order (``layout="xyz"``) or (ny, nx, nz) columns (``layout="columns"``, the
+kernels' native order, no conversion); 4D volumes carry a leading gate
+axis.  Detector stacks are (nviews, nv, nu).  Results are accumulated into
+``out`` when it is given, as in the reference (the caller zeroes it).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .footprint import FootprintTable
+from .geometry import Scan3D, TRTT_CONE_BEAM, TRTT_FAN_BEAM, TRTT_PARALLEL_BEAM
+
+LAYOUTS = {"xyz": 0, "columns": 1}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream):
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Projector3D:
+    """All views of a 3D parallel / cone beam scan on one GPU.
+
+    ``table`` selects the tabulated footprint (``trtt_PB3D``/``trtt_CB3D``);
+    ``None`` the closed-form cubic one (``trtt_PB3D_cubic``/``trtt_CB3D_cubic``).
+    """
+
+    def __init__(self, scan: Scan3D, table: FootprintTable | None = None,
+                 device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise _lib.TrttError("Projector3D needs a CUDA device (no CPU fallback)")
+        self.scan = scan
+        self.table = table
+        self.device = torch.device("cuda", torch.cuda.current_device()
+                                   if device is None else torch.device(device).index or 0)
+        self.nt = 1
+        lib = _lib.load()
+        xos = np.ascontiguousarray(scan.xos, dtype=np.float64)
+        xsd = np.ascontiguousarray(scan.xsd, dtype=np.float64)
+        handle = C.c_void_p()
+        geom = {TRTT_PARALLEL_BEAM: 3, TRTT_CONE_BEAM: 4, TRTT_FAN_BEAM: 5}[scan.mode]
+        with torch.cuda.device(self.device):
+            if table is None:
+                rc = lib.trtt_b200_plan3d_create(
+                    C.byref(handle), geom, scan.nx, scan.ny, scan.nz, scan.s_scl,
+                    scan.s_deg, None, 0, 1.0, None, scan.nu, scan.nv, scan.u_scl,
+                    scan.v_scl, scan.nviews, _lib.dptr(xos), _lib.dptr(xsd))
+            else:
+                rc = lib.trtt_b200_plan3d_create(
+                    C.byref(handle), geom, scan.nx, scan.ny, scan.nz, scan.s_scl,
+                    scan.s_deg, _lib.dptr(table.cum), table.size, table.step,
+                    _lib.dptr(table.coord), scan.nu, scan.nv, scan.u_scl, scan.v_scl,
+                    scan.nviews, _lib.dptr(xos), _lib.dptr(xsd))
+        _lib.check(rc, "trtt_b200_plan3d_create")
+        self._h = handle
+
+    # -- configuration -------------------------------------------------------
+    def set_gates(self, nt: int, t_index) -> None:
+        """4D: view k projects the linear interpolation of gates floor/ceil of
+        t_index[k] (Ytrtt_3D_projectors.i:301-311)."""
+        t = np.ascontiguousarray(t_index, dtype=np.float64)
+        if t.shape != (self.scan.nviews,):
+            raise ValueError("t_index must have one entry per view")
+        _lib.check(_lib.load().trtt_b200_plan3d_set_gates(self._h, nt, _lib.dptr(t)),
+                   "trtt_b200_plan3d_set_gates")
+        self.nt = int(nt)
+
+    def set_tiles(self, band_rows: int = 0, warps: int = 0) -> None:
+        _lib.check(_lib.load().trtt_b200_plan3d_set_tiles(self._h, band_rows, warps),
+                   "trtt_b200_plan3d_set_tiles")
+
+    @property
+    def factorized(self) -> bool:
+        return bool(_lib.load().trtt_b200_plan3d_factorized(self._h))
+
+    # -- shapes ---------------------------------------------------------------
+    def volume_shape(self, layout="xyz"):
+        s = self.scan
+        base = (s.nz, s.ny, s.nx) if layout == "xyz" else (s.ny, s.nx, s.nz)
+        return ((self.nt,) + base) if self.nt > 1 else base
+
+    def detector_shape(self, nviews=None):
+        s = self.scan
+        return (s.nviews if nviews is None else nviews, s.nv, s.nu)
+
+    def _check(self, t, shape, name):
+        torch = _torch()
+        if not isinstance(t, torch.Tensor) or t.device.type != "cuda" or t.dtype != torch.float32:
+            raise TypeError(f"{name} must be a float32 CUDA tensor")
+        if tuple(t.shape) != tuple(shape) or not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous with shape {tuple(shape)}, got {tuple(t.shape)}")
+
+    # -- application ------------------------------------------------------------
+    def forward(self, vol, out=None, view0: int = 0, nview: int | None = None,
+                layout: str = "xyz", stream=None):
+        """out[v] += H_v vol for views [view0, view0+nview)."""
+        torch = _torch()
+        nview = self.scan.nviews - view0 if nview is None else nview
+        self._check(vol, self.volume_shape(layout), "vol")
+        if out is None:
+            out = torch.zeros(self.detector_shape(nview), dtype=torch.float32, device=vol.device)
+        self._check(out, self.detector_shape(nview), "out")
+        rc = _lib.load().trtt_b200_plan3d_forward(
+            self._h, C.c_void_p(vol.data_ptr()), C.c_void_p(out.data_ptr()), view0, nview,
+            LAYOUTS[layout], _stream_ptr(stream))
+        _lib.check(rc, "trtt_b200_plan3d_forward")
+        return out
+
+    def backward(self, sino, out=None, view0: int = 0, nview: int | None = None,
+                 layout: str = "xyz", stream=None):
+        """out += sum_v H_v^T sino[v] over views [view0, view0+nview)."""
+        torch = _torch()
+        nview = self.scan.nviews - view0 if nview is None else nview
+        self._check(sino, self.detector_shape(nview), "sino")
+        if out is None:
+            out = torch.zeros(self.volume_shape(layout), dtype=torch.float32, device=sino.device)
+        self._check(out, self.volume_shape(layout), "out")
+        rc = _lib.load().trtt_b200_plan3d_backward(
+            self._h, C.c_void_p(sino.data_ptr()), C.c_void_p(out.data_ptr()), view0, nview,
+            LAYOUTS[layout], _stream_ptr(stream))
+        _lib.check(rc, "trtt_b200_plan3d_backward")
+        return out
+
+    def __call__(self, x, job: int = 0, **kw):
+        """Yorick-style evaluator C(x, job): job 0 direct, 1 transpose."""
+        if job == 0:
+            return self.forward(x, **kw)
+        if job == 1:
+            return self.backward(x, **kw)
+        raise ValueError("unsupported job (0 = direct, 1 = transpose)")
+
+    def status(self, stream=None) -> None:
+        """Raise if a kernel flagged an error (a voxel in the source plane)."""
+        _lib.check(_lib.load().trtt_b200_plan3d_status(self._h, _stream_ptr(stream)),
+                   "projector")
+
+    def single_view(self, k: int):
+        """Per-view closure ``A_single_3D`` (Ytrtt_3D_projectors.i:56-138)."""
+        def op(x, job=0, **kw):
+            return self(x, job, view0=k, nview=1, **kw)
+        return op
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().trtt_b200_plan3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def columns_from_xyz(vol):
+    """(…, nz, ny, nx) -> (…, ny, nx, nz) (reference order to kernel order)."""
+    return vol.movedim(-3, -1).contiguous()
+
+
+def xyz_from_columns(vol):
+    """(…, ny, nx, nz) -> (…, nz, ny, nx)."""
+    return vol.movedim(-1, -3).contiguous()
