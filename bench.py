@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Projector-pair throughput on B200: cone-beam 256^3 -> 360 x 512^2.
+
+One step = the forward projection of all 360 views of a 256^3 FP32 volume
+(closed-form cubic B-spline footprint, SID 1000 mm, SDD 1500 mm, 1 mm
+voxels and detector cells) followed by the transpose of all 360 views: the
+data-fidelity operator pair of one reconstruction iteration.  The metric
+counts each per-view forward and each per-view transpose as one projection
+(views * 2 per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank projects its own 360-view scan (views
+are independent units, weak scaling, no data-path collective); the timing
+is the maximum over ranks.  Rank 0 prints one JSON line.
+
+``--impl reference`` times the reference plugin C (compiled from its
+sources into oracle/_ref, FP64, single-threaded per call) on the host
+cores, views spread over all available threads, on a bounded sample of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+ND = 512
+VIEWS = 360
+SID, SDD = 1000.0, 1500.0
+WORKLOAD = (f"cone-beam circular orbit, {N}^3 FP32 volume of 20 random ellipsoids -> "
+            f"{VIEWS} x {ND}x{ND} detector, 1 mm voxels/cells, SID {SID:g} mm, SDD {SDD:g} mm, "
+            "closed-form cubic B-spline footprint; step = forward + transpose of all views")
+
+
+def _env_int(name, default):
+    v = os.environ.get(name)
+    return int(v) if v is not None else default
+
+
+def scan(rank=0, views=VIEWS):
+    from yoricktrtt_b200 import geometry as G
+    theta0 = rank * (2 * math.pi / views) / max(1, _env_int("WORLD_SIZE", 1))
+    th = theta0 + np.arange(views) * (2 * math.pi / views)
+    return G.circular_scan_3d(N, N, N, 1.0, 3, ND, ND, 1.0, 1.0, views,
+                              mode=G.TRTT_CONE_BEAM, rsc=SID, rsd=SDD, theta=th)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference plugin (or the oracle port) on host threads
+# ---------------------------------------------------------------------------
+def cpu_pair_sample(nviews_sample, threads=None):
+    """Time nviews_sample forward+transpose view pairs of the workload with the
+    reference C on `threads` host threads (views spread over threads, private
+    outputs, as the reference's MPY decomposition does).  Returns
+    (projections/s, seconds, kind, threads)."""
+    from oracle import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    orc = oracle.get("ref" if kind == "reference" else "port")
+    from yoricktrtt_b200 import phantoms as P
+    sc = scan(0, VIEWS)
+    vol = np.ascontiguousarray(P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float64))
+    det_in = np.ascontiguousarray(np.random.default_rng(0).random((ND, ND)))
+    threads = threads or (os.cpu_count() or 1)
+    threads = max(1, min(threads, nviews_sample))
+    views = np.linspace(0, VIEWS - 1, nviews_sample).astype(int)
+
+    def work(vs):
+        for v in vs:
+            out = np.zeros((ND, ND))
+            orc.cb3d(out, vol, sc, int(v), 0)
+            back = np.zeros_like(vol)
+            orc.cb3d(back, det_in, sc, int(v), 1)
+
+    chunks = [views[t::threads] for t in range(threads)]
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work, args=(c,)) for c in chunks]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    return 2 * nviews_sample / dt, dt, kind, threads
+
+
+def run_reference(args):
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    try:
+        from oracle import oracle
+        oracle.build(ref=True)
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle build failed: {e}"}))
+        return 0
+    cores = os.cpu_count() or 1
+    sample = max(1, min(cores, 8))
+    times = []
+    for it in range(args.warmup + args.steps):
+        val, dt, kind, thr = cpu_pair_sample(sample, cores)
+        if it >= args.warmup:
+            times.append(dt)
+    dt = statistics.median(times)
+    value = 2 * sample / dt
+    line = {
+        "impl": "reference", "metric": "fwd+back projections/s", "value": value,
+        "unit": "projections/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{sample} of {VIEWS} view pairs per step"},
+        "cpu_baseline": {"value": value, "unit": "projections/s", "cores": thr, "kind": kind,
+                         "sample": f"{sample} view pairs (forward + transpose) of the workload, "
+                                   f"views spread over {thr} threads"},
+        "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from yoricktrtt_b200 import _lib, phantoms as P
+    from yoricktrtt_b200.projectors import Projector3D, columns_from_xyz
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    sc = scan(rank)
+    pr = Projector3D(sc)
+    if args.band_rows or args.warps:
+        pr.set_tiles(args.band_rows, args.warps)
+    vol_h = P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float32)
+    x = columns_from_xyz(torch.tensor(vol_h, device=dev))
+    sino = torch.zeros(VIEWS, ND, ND, device=dev)
+    back = torch.zeros_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        sino.zero_()
+        back.zero_()
+        if ev:
+            ev[0].record(stream)
+        pr.forward(x, out=sino, layout="columns")
+        if ev:
+            ev[1].record(stream)
+        pr.backward(sino, out=back, layout="columns")
+        if ev:
+            ev[2].record(stream)
+        flush.fill_(1.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    pr.status()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = _lib.launch_count()
+    with ClockSampler(local) as clk:
+        barrier()
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t_end.record(stream)
+        barrier()
+    launches = _lib.launch_count() - launches0
+    ms = t_start.elapsed_time(t_end)
+    fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    back_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pr.status()
+    total_proj = 2 * VIEWS * world * args.steps
+    value = total_proj / (ms / 1e3)
+
+    # roofline of the dominant kernel: algorithmic bytes per launch (per-view
+    # streaming model: the forward reads the volume and writes one detector
+    # image per view, the transpose reads one image and writes the volume
+    # contribution per view) / measured launch duration
+    nvox, npix = N ** 3, ND * ND
+    fwd_avg, back_avg = statistics.mean(fwd_ms), statistics.mean(back_ms)
+    if back_avg >= fwd_avg:
+        kern, kms = "k_back3d_col (transpose, column gather)", back_avg
+    else:
+        kern, kms = "k_fwd3d_band (direct, detector-row bands)", fwd_avg
+    alg_bytes = VIEWS * (4 * nvox + 4 * npix)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (kms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            tr = json.load(f)
+        traffic = tr.get(kern.split()[0])
+    except Exception:
+        pass
+
+    # end to end through the batched host-buffer C ABI (host FP64 arrays in
+    # the reference layouts, copies inside the timed region)
+    e2e = None
+    if rank == 0 and not args.skip_e2e:
+        e2e = run_e2e(sc, vol_h, args, dev)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        try:
+            val, dt, kind, thr = cpu_pair_sample(max(1, min(os.cpu_count() or 1, 8)))
+            cpu = {"value": val, "unit": "projections/s", "cores": thr, "kind": kind,
+                   "sample": f"{min(os.cpu_count() or 1, 8)} view pairs (forward + transpose) of the "
+                             f"workload, reference C in FP64, one view per thread ({dt:.1f} s)"}
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "unit": "projections/s", "cores": 0, "kind": "port",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "fwd+back projections/s", "value": value, "unit": "projections/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "views_per_gpu": VIEWS, "volume": [N, N, N],
+                       "detector": [ND, ND], "footprint": "cubic",
+                       "l2": "256 MiB buffer written between steps (inside the timed region); "
+                             "the 360-view detector stack (377 MB) exceeds L2",
+                       "fwd_ms": fwd_avg, "back_ms": back_avg,
+                       "band_rows": args.band_rows or "auto"},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(sc, vol_h, args, dev):
+    """The same pair through trtt_b200_cb3d_batch on pinned host FP64 arrays."""
+    import torch
+    from yoricktrtt_b200 import _lib
+    lib = _lib.load()
+    vol64 = torch.from_numpy(np.ascontiguousarray(vol_h, dtype=np.float64)).pin_memory().numpy()
+    det = torch.zeros((VIEWS, ND, ND), dtype=torch.float64).pin_memory().numpy()
+    back = torch.zeros((N, N, N), dtype=torch.float64).pin_memory().numpy()
+    xos = np.ascontiguousarray(sc.xos)
+    xsd = np.ascontiguousarray(sc.xsd)
+
+    def call(out, inp, job):
+        rc = lib.trtt_b200_cb3d_batch(_lib.dptr(out), _lib.dptr(inp), N, N, N, 1.0, 3, None, 0,
+                                      1.0, None, ND, ND, 1.0, 1.0, VIEWS, _lib.dptr(xos),
+                                      _lib.dptr(xsd), 4, job)
+        _lib.check(rc, "trtt_b200_cb3d_batch")
+
+    def step():
+        det.fill(0.0)
+        back.fill(0.0)
+        call(det, vol64, 0)
+        call(back, det, 1)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / steps
+    nvox, npix = N ** 3, ND * ND * VIEWS
+    # per step: forward copies in (volume) and out (detector) to the device and
+    # out back; transpose copies in (detector) and out (volume) and out back
+    h2d = 8 * (nvox + npix) + 8 * (npix + nvox)
+    d2h = 8 * npix + 8 * nvox
+    return {"value": 2 * VIEWS / dt, "unit": "projections/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
+            "path": "trtt_b200_cb3d_batch (host FP64 arrays, reference layouts, pinned)"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--band-rows", type=int, default=0)
+    ap.add_argument("--warps", type=int, default=0)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -195,6 +195,41 @@ int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
 
 int trtt_b200_plan3d_destroy(trtt_b200_plan3d *plan);
 
+typedef struct trtt_b200_plan2d trtt_b200_plan2d;
+
+/* 2D B-spline projector plan (trtt_PB2D/FB2D geometry and footprint
+ * semantics, plugin/trtt_2D_projectors.c:186-383) for `nviews` views;
+ * cum_footprint == NULL selects the closed-form cubic footprint
+ * (trtt_PB2D_cubic/trtt_FB2D_cubic). */
+int trtt_b200_plan2d_create(trtt_b200_plan2d **plan, int geometry, long nx, long ny,
+                            double s_scl, int s_deg, const double *cum_footprint,
+                            long size_footprint, double step_footprint,
+                            const double *coord_footprint, long nv, double v_scl,
+                            long nviews, const double *xos, const double *xsd);
+
+/* Long-Fessler plan: `params` is a trtt_b200_lf2d_parameters block, one
+ * (beta, detector offset) pair per view (LongFessler2D.c:41-470). */
+int trtt_b200_plan2d_create_lf(trtt_b200_plan2d **plan, const void *params,
+                               int line_integ, long nviews, const double *beta,
+                               const double *offset);
+
+/* sino[view][nv] += H img  /  img += H^T sino  (img is [j][i], nx fastest). */
+int trtt_b200_plan2d_forward(trtt_b200_plan2d *plan, const float *img, float *sino,
+                             void *stream);
+int trtt_b200_plan2d_backward(trtt_b200_plan2d *plan, const float *sino, float *img,
+                              void *stream);
+int trtt_b200_plan2d_status(trtt_b200_plan2d *plan, void *stream);
+
+/* GPU assembly of the per-view sparse system matrices as 1-based COO
+ * triplets (the matrix the reference builds column by column with the
+ * sparsers, Ytrtt_2D_projectors.i:212-369).  Device arrays of
+ * nviews*nx*ny*max_cells entries; slot ((view*nx*ny)+pixel)*max_cells+l;
+ * unused slots have row = col = 0. */
+int trtt_b200_plan2d_assemble(trtt_b200_plan2d *plan, int max_cells, double *a,
+                              long *rows, long *cols, void *stream);
+
+int trtt_b200_plan2d_destroy(trtt_b200_plan2d *plan);
+
 /* Batched host-buffer entry point: the whole scan in one call.  Same
  * conventions as trtt_CB3D/trtt_CB3D_cubic (host double*, accumulate,
  * reference layouts) for `nviews` views: xos/xsd are nviews*12, the

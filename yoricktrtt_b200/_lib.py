@@ -55,6 +55,14 @@ SIGNATURES = {
     "trtt_b200_plan3d_set_tiles": (_I, [_vp, _I, _I]),
     "trtt_b200_plan3d_factorized": (_I, [_vp]),
     "trtt_b200_plan3d_destroy": (_I, [_vp]),
+    "trtt_b200_plan2d_create": (_I, [C.POINTER(_vp), _I, _L, _L, _D, _I, _dp, _L, _D, _dp, _L,
+                                      _D, _L, _dp, _dp]),
+    "trtt_b200_plan2d_create_lf": (_I, [C.POINTER(_vp), _vp, _I, _L, _dp, _dp]),
+    "trtt_b200_plan2d_forward": (_I, [_vp, _vp, _vp, _vp]),
+    "trtt_b200_plan2d_backward": (_I, [_vp, _vp, _vp, _vp]),
+    "trtt_b200_plan2d_status": (_I, [_vp, _vp]),
+    "trtt_b200_plan2d_assemble": (_I, [_vp, _I, _vp, _vp, _vp, _vp]),
+    "trtt_b200_plan2d_destroy": (_I, [_vp]),
     "trtt_b200_cb3d_batch": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
                                    _D, _L, _dp, _dp, _I, _I]),
 }
