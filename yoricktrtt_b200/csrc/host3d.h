@@ -1,0 +1,121 @@
+// host3d.h -- host-side derivation of the 3D projector parameters shared by
+// the C ABI translation units (plan, drop-in and allocation-free entry
+// points).
+#pragma once
+
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+#include "../../include/trtt_b200.h"
+
+namespace trtt {
+
+// Per-view constants of the 3D projectors, derived in FP64 with the operand
+// order of the reference so that the device sees the reference's values
+// (cone beam plugin/trtt_3D_projectors.c:1186-1230, parallel beam
+// plugin/trtt_3D_projectors.c:963-1004; identical in the _cubic file).
+inline void make_view3d(const Params3D &P, const double *xos, const double *xsd, View3D &V)
+{
+  std::memset(&V, 0, sizeof(V));
+  const double a1 = xsd[0], a2 = xsd[1], a3 = xsd[2], a4 = xsd[3];
+  const double a5 = xsd[4], a6 = xsd[5], a7 = xsd[6], a8 = xsd[7];
+  const double a9 = xsd[8], a10 = xsd[9], a11 = xsd[10], a12 = xsd[11];
+  const double o1 = xos[0], o2 = xos[1], o3 = xos[2], o4 = xos[3];
+  const double o5 = xos[4], o6 = xos[5], o7 = xos[6], o8 = xos[7];
+  const double o9 = xos[8], o10 = xos[9], o11 = xos[10], o12 = xos[11];
+  const double a1inv = -1.0 * (1.0 / a1);
+  const double b1 = a6 + a1inv * a5 * a2, c1 = a10 + a1inv * a9 * a2;
+  const double b2 = a7 + a1inv * a5 * a3, c2 = a11 + a1inv * a9 * a3;
+  const double b3 = a8 + a1inv * a5 * a4, c3 = a12 + a1inv * a9 * a4;
+  V.o1 = o1; V.o2 = o2; V.o3 = o3; V.o4 = o4;
+  V.nv_x = b1 * o5 + b2 * o9;  V.nu_x = c1 * o5 + c2 * o9;
+  V.nv_y = b1 * o6 + b2 * o10; V.nu_y = c1 * o6 + c2 * o10;
+  V.nv_z = b1 * o7 + b2 * o11; V.nu_z = c1 * o7 + c2 * o11;
+  V.nv_c = b1 * o8 + b2 * o12; V.nu_c = c1 * o8 + c2 * o12;
+  V.d_x = a1 * o1 + a2 * o5 + a3 * o9;
+  V.d_y = a1 * o2 + a2 * o6 + a3 * o10;
+  V.d_z = a1 * o3 + a2 * o7 + a3 * o11;
+  V.d_c = a1 * o4 + a2 * o8 + a3 * o12;
+  V.a4sqr = a4 * a4;
+  V.a4m = -1.0 * a4;
+  V.a8 = a8;
+  V.a12 = a12;
+  V.b3 = b3;
+  V.c3 = c3;
+  // parallel beam
+  V.v_x = b1 * o5 + b2 * o9;  V.u_x = c1 * o5 + c2 * o9;
+  V.v_y = b1 * o6 + b2 * o10; V.u_y = c1 * o6 + c2 * o10;
+  V.v_z = b1 * o7 + b2 * o11; V.u_z = c1 * o7 + c2 * o11;
+  V.v_c = b1 * o8 + b2 * o12 + b3; V.u_c = c1 * o8 + c2 * o12 + c3;
+  const double a1sqr = a1 * a1;
+  const double a5sqr = P.v_scl * P.v_scl * a5 * a5;
+  const double a9sqr = P.u_scl * P.u_scl * a9 * a9;
+  const double delta_u = std::sqrt(1.0 + (a9sqr / (a1sqr + a5sqr)));
+  const double delta_v = std::sqrt(1.0 + (a5sqr / a1sqr));
+  V.p_rho0 = P.s_scl * P.s_scl * P.s_scl * delta_u * delta_v;
+  V.p_h_u = P.s_scl / P.u_scl;
+  V.p_h_v = P.s_scl / P.v_scl;
+  V.p_scl_u = 1.0 / V.p_h_u;
+  V.p_scl_v = 1.0 / V.p_h_v;
+  V.p_hs_u = P.hs0 * V.p_h_u;
+  V.p_hs_v = P.hs0 * V.p_h_v;
+  V.p_sclt_u = V.p_scl_u / P.step;
+  V.p_sclt_v = V.p_scl_v / P.step;
+  V.g0 = 0;
+  V.g1 = 0;
+  V.w0 = 1.0f;
+  V.w1 = 0.0f;
+  if (P.geom == GEOM_CONE)
+    V.factorized = (V.o3 == 0.0 && V.d_z == 0.0 && V.nv_z == 0.0) ? 1 : 0;
+  else
+    V.factorized = (V.v_z == 0.0) ? 1 : 0;
+}
+
+inline Params3D make_params(int geom, long nx, long ny, long nz, double s_scl, int s_deg,
+                     const double *cum_dev, long size, double step,
+                     double coord0, long nu, long nv, double u_scl, double v_scl)
+{
+  Params3D P;
+  std::memset(&P, 0, sizeof(P));
+  P.geom = geom;
+  P.model = cum_dev ? MODEL_TABLE : MODEL_CUBIC;
+  P.nx = (int)nx; P.ny = (int)ny; P.nz = (int)nz;
+  P.nu = (int)nu; P.nv = (int)nv;
+  P.nt = 1;
+  P.s_scl = s_scl;
+  P.u_scl = u_scl;
+  P.v_scl = v_scl;
+  P.rho0_init = s_scl * s_scl * s_scl;
+  P.h_u0 = s_scl / u_scl;
+  P.h_v0 = s_scl / v_scl;
+  P.hs0 = 0.5 * (s_deg + 1);
+  P.cum = cum_dev;
+  P.size = (int)size;
+  P.last = (double)(size - 1);
+  P.step = cum_dev ? step : 1.0;
+  P.coord0 = coord0;
+  return P;
+}
+
+// Band shape of the direct kernel for a detector nu cells wide.
+inline void choose_band(int nu, int nv, int &band_rows, int &warps)
+{
+  const long budget = 200 * 1024;
+  warps = 16;
+  while (warps > 2 && (long)warps * nu * 4 > budget / 3) warps /= 2;
+  const long rest = budget - (long)warps * nu * 4;
+  long rows = rest / ((long)nu * 4 + (long)warps * 4);
+  if (rows > 64) rows = 64;
+  if (rows > nv) rows = nv;
+  band_rows = rows >= 2 ? (int)rows : 0;
+}
+
+inline int geom_code(int geometry)
+{
+  if (geometry == TRTT_B200_PARALLEL_BEAM) return GEOM_PARALLEL;
+  if (geometry == TRTT_B200_CONE_BEAM || geometry == TRTT_B200_FAN_BEAM) return GEOM_CONE;
+  return -1;
+}
+
+}  // namespace trtt
