@@ -185,9 +185,13 @@ int trtt_b200_plan3d_backward(trtt_b200_plan3d *plan, const float *sino,
  * an error since the last call, -1 otherwise (flags are cleared). */
 int trtt_b200_plan3d_status(trtt_b200_plan3d *plan, void *stream);
 
-/* Override the direct-projector band kernel shape (detector rows per CTA
- * and warps per CTA); 0 keeps the current value.  band_rows < 0 forces the
- * per-voxel kernel. */
+/* Direct-projector kernel selection.  (0, 0): defaults (band kernel with
+ * shared-memory accumulation, automatic shape).  band_rows > 0: band kernel
+ * with that many detector rows per CTA and `warps` warps per CTA (0 keeps
+ * the current value).  band_rows == TRTT_B200_TILES_PULL: closed-form model,
+ * atomic-free band kernel (each detector cell accumulated in registers by one
+ * owning thread; nu <= 512).  Other band_rows < 0: the per-voxel kernel. */
+#define TRTT_B200_TILES_PULL (-2)
 int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps);
 
 /* 1 if every view of the plan uses the column-factorised kernels. */

@@ -176,7 +176,7 @@ def test_view_subrange_and_tiles(oracle_port):
     pr = Projector3D(sc)
     xt = torch.tensor(vol, dtype=torch.float32, device="cuda")
     full = pr.forward(xt).cpu().numpy()
-    for rows, warps in [(4, 2), (7, 4), (36, 16), (-1, 0)]:
+    for rows, warps in [(4, 2), (7, 4), (36, 16), (-1, 0), (-2, 0), (0, 0)]:
         pr.set_tiles(rows, warps)
         part = pr.forward(xt, view0=2, nview=3).cpu().numpy()
         assert rel_l2(part, full[2:5]) <= 1e-6, (rows, warps)

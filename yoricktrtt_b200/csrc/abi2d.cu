@@ -13,7 +13,7 @@
 
 #include "kernels2d.h"
 #include "runtime.h"
-#include "../../include/trtt_b200.h"
+#include "trtt_b200.h"
 
 using namespace trtt;
 

@@ -12,7 +12,7 @@
 #include "host3d.h"
 #include "kernels.h"
 #include "runtime.h"
-#include "../../include/trtt_b200.h"
+#include "trtt_b200.h"
 
 using namespace trtt;
 
@@ -26,6 +26,7 @@ struct trtt_b200_plan3d {
   long nviews = 0;
   int nt = 1;
   int band_rows = 0, warps = 16;
+  int pull = 0;  // 1: atomic-free band kernel (closed-form model, nu <= 512)
   bool factorized = true;
   DevBuf views, cum, gate_ptr, entries, scratch, err;
   std::vector<View3D> hviews;
@@ -149,6 +150,16 @@ extern "C" int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *pl, int band_rows, i
 {
   clear_error();
   if (!pl) return fail("plan3d_set_tiles: null plan");
+  if (band_rows == 0 && warps == 0) {  // defaults
+    pl->pull = 0;
+    choose_band(pl->P.nu, pl->P.nv, pl->band_rows, pl->warps);
+    return 0;
+  }
+  if (band_rows == TRTT_B200_TILES_PULL) {  // atomic-free band kernel
+    pl->pull = 1;
+    return 0;
+  }
+  pl->pull = 0;
   if (warps > 0) {
     if (warps < 2 || warps > 16) return fail("plan3d_set_tiles: warps must be in [2, 16]");
     pl->warps = warps;
@@ -205,6 +216,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
     L.sino_view_stride = npix;
     L.band_rows = pl->factorized ? pl->band_rows : 0;
     L.warps = pl->warps;
+    L.pull = pl->pull;
     L.err = pl->err.as<int>();
     TRTT_CK(launch_fwd3d(L, st));
     count_launch();

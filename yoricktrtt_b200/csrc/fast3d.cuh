@@ -1,0 +1,77 @@
+// fast3d.cuh -- packed-FP32 (f32x2) evaluation of the closed-form cubic
+// footprint for two voxels at a time (sm_100a FFMA2/FMUL2/FADD2).
+//
+// The direct and transpose kernels of the cubic model both call
+// voxel_u_pair() and cubic_prim2(), so the pair stays an exact adjoint.
+#pragma once
+
+#include "geom3d.cuh"
+
+namespace trtt {
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// Cubic B-spline primitive at two abscissae.  With t = |x| the tail mass
+// beyond t is g(t) = ((2-t)_+^4 - 4 (1-t)_+^4) / 24 (truncated-power form of
+// the centred cubic B-spline), and P(x) = 1/2 + sign(x) (1/2 - g(|x|)).
+// Expanding gives the four quartics of
+// plugin/trtt_3D_projectors_cubic.c:117-138; agreement is to FP32 rounding.
+__device__ __forceinline__ float2 cubic_prim2(float2 x)
+{
+  const float2 t = make_float2(fabsf(x.x), fabsf(x.y));
+  float2 a = fma2(t, f2(-1.0f), f2(2.0f));
+  float2 b = fma2(t, f2(-1.0f), f2(1.0f));
+  a = make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f));
+  b = make_float2(fmaxf(b.x, 0.0f), fmaxf(b.y, 0.0f));
+  const float2 a2 = mul2(a, a), b2 = mul2(b, b);
+  const float2 a4 = mul2(a2, a2), b4 = mul2(b2, b2);
+  const float2 g = fma2(a4, f2(0.0416666666666667f), mul2(b4, f2(-0.1666666666666667f)));
+  const float2 h = fma2(g, f2(-1.0f), f2(0.5f));  // 1/2 - g
+  return add2(make_float2(copysignf(h.x, x.x), copysignf(h.y, x.y)), f2(0.5f));
+}
+
+// u-footprints of two voxels of one column (closed-form model): cells
+// [lo, lo+n) and edge abscissae start + l*inc, weighting factors rho.
+struct UPair {
+  int lo0, n0, lo1, n1;
+  float2 start, inc, rho;
+};
+
+template <int GEOM>
+__device__ __forceinline__ void voxel_u_pair(const Params3D &P, const View3D &V,
+                                             const ColGeo<MODEL_CUBIC> &c, int k0, int k1,
+                                             UPair &up)
+{
+  const double uc0 = fma(c.B, (double)k0, c.A);
+  const double uc1 = fma(c.B, (double)k1, c.A);
+  float2 scl, hs;
+  if constexpr (GEOM == GEOM_CONE) {
+    const float2 d = make_float2((float)(uc0 - V.a12), (float)(uc1 - V.a12));
+    const float2 uca = mul2(d, f2((float)P.u_scl));
+    const float2 du2 = fma2(mul2(uca, uca), f2(c.inv_den), f2(1.0f));
+    const float2 dlt = mul2(du2, make_float2(rsqrtf(du2.x), rsqrtf(du2.y)));
+    const float2 h = mul2(dlt, f2(c.h_u0m));
+    scl = make_float2(__frcp_rn(h.x), __frcp_rn(h.y));
+    hs = mul2(h, f2((float)P.hs0));
+    up.rho = mul2(dlt, f2(c.rho0c));
+  } else {
+    scl = f2((float)V.p_scl_u);
+    hs = f2((float)V.p_hs_u);
+    up.rho = f2((float)V.p_rho0);
+  }
+  const int n = P.nu;
+  up.lo0 = clamp_left_cell(uc0 - (double)hs.x, n);
+  up.n0 = clamp_right_cell(uc0 + (double)hs.x, n - 1) - up.lo0;
+  up.lo1 = clamp_left_cell(uc1 - (double)hs.y, n);
+  up.n1 = clamp_right_cell(uc1 + (double)hs.y, n - 1) - up.lo1;
+  const float2 off = make_float2((float)((double)up.lo0 - uc0), (float)((double)up.lo1 - uc1));
+  up.start = mul2(off, scl);
+  up.inc = scl;
+  if (!(isfinite(up.start.x) && isfinite(scl.x))) up.n0 = 0;
+  if (!(isfinite(up.start.y) && isfinite(scl.y))) up.n1 = 0;
+}
+
+}  // namespace trtt

@@ -7,7 +7,7 @@
 #include <cstring>
 
 #include "kernels.h"
-#include "../../include/trtt_b200.h"
+#include "trtt_b200.h"
 
 namespace trtt {
 
@@ -106,7 +106,7 @@ inline void choose_band(int nu, int nv, int &band_rows, int &warps)
   while (warps > 2 && (long)warps * nu * 4 > budget / 3) warps /= 2;
   const long rest = budget - (long)warps * nu * 4;
   long rows = rest / ((long)nu * 4 + (long)warps * 4);
-  if (rows > 64) rows = 64;
+  if (rows > 32) rows = 32;  // two CTAs (2 x 16 warps) per SM at nu = 512
   if (rows > nv) rows = nv;
   band_rows = rows >= 2 ? (int)rows : 0;
 }

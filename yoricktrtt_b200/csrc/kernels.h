@@ -30,6 +30,7 @@ struct Fwd3DLaunch {
   long sino_view_stride; // nv*nu
   int band_rows;         // > 0: band kernel (factorised views); 0: per-voxel
   int warps;             // warps per CTA of the band kernel
+  int pull = 0;          // closed-form model, nu <= 512: atomic-free band kernel
   int *err;              // device error flags
 };
 
@@ -50,6 +51,9 @@ struct Back3DLaunch {
 
 cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st);
 cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st);
+// closed-form model on factorised views, packed FP32x2 (proj3d_fast.cu)
+cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st);
+cudaError_t launch_back3d_fast(const Back3DLaunch &L, cudaStream_t st);
 
 // Layout / precision conversions (convert.cu).
 // XYZ layout is the reference's [k][j][i] (x fastest); column layout is

@@ -31,7 +31,7 @@
 #include "host3d.h"
 #include "kernels.h"
 #include "runtime.h"
-#include "../../include/trtt_b200.h"
+#include "trtt_b200.h"
 
 using namespace trtt;
 

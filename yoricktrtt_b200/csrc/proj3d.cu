@@ -433,6 +433,7 @@ static cudaError_t launch_back(const Back3DLaunch &L, cudaStream_t st)
 
 cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st)
 {
+  if (L.P.model == MODEL_CUBIC && L.band_rows > 0) return launch_fwd3d_fast(L, st);
   if (L.P.geom == GEOM_CONE)
     return L.P.model == MODEL_TABLE ? launch_fwd<GEOM_CONE, MODEL_TABLE>(L, st)
                                     : launch_fwd<GEOM_CONE, MODEL_CUBIC>(L, st);
@@ -442,6 +443,7 @@ cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st)
 
 cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st)
 {
+  if (L.P.model == MODEL_CUBIC && L.factorized) return launch_back3d_fast(L, st);
   if (L.P.geom == GEOM_CONE)
     return L.P.model == MODEL_TABLE ? launch_back<GEOM_CONE, MODEL_TABLE>(L, st)
                                     : launch_back<GEOM_CONE, MODEL_CUBIC>(L, st);

@@ -1,0 +1,531 @@
+// proj3d_fast.cu -- closed-form (cubic) 3D projector pair for column-
+// factorised views, two voxels per lane with packed FP32x2 arithmetic.
+//
+// Same decomposition as proj3d.cu (direct: detector-row bands in shared
+// memory; transpose: one warp per voxel column gathering through the
+// column's v-collapsed detector profile), but every lane handles voxel pairs
+// (k, k+32) so that the footprint scales and the B-spline primitive of both
+// voxels are evaluated by the same FFMA2/FMUL2/FADD2 instructions
+// (fast3d.cuh).
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "fast3d.cuh"
+#include "kernels.h"
+
+namespace trtt {
+
+static constexpr unsigned FULLM = 0xffffffffu;
+
+__device__ __forceinline__ ColGeo<MODEL_CUBIC> shfl_colc(const ColGeo<MODEL_CUBIC> &c, int src)
+{
+  ColGeo<MODEL_CUBIC> r;
+  r.vax.lo = __shfl_sync(FULLM, c.vax.lo, src);
+  r.vax.n = __shfl_sync(FULLM, c.vax.n, src);
+  r.vax.start = __shfl_sync(FULLM, c.vax.start, src);
+  r.vax.inc = __shfl_sync(FULLM, c.vax.inc, src);
+  r.bad = 0;
+  r.A = __shfl_sync(FULLM, c.A, src);
+  r.B = __shfl_sync(FULLM, c.B, src);
+  r.h_u0m = __shfl_sync(FULLM, c.h_u0m, src);
+  r.rho0c = __shfl_sync(FULLM, c.rho0c, src);
+  r.inv_den = __shfl_sync(FULLM, c.inv_den, src);
+  return r;
+}
+
+__device__ __forceinline__ float vox_val(const float *__restrict__ vol, long gate_stride,
+                                         const View3D &V, long idx)
+{
+  float x = __ldg(vol + (long)V.g0 * gate_stride + idx);
+  if (V.w1 != 0.0f) return fmaf(V.w0, x, V.w1 * __ldg(vol + (long)V.g1 * gate_stride + idx));
+  return V.w0 == 1.0f ? x : V.w0 * x;
+}
+
+// ---------------------------------------------------------------------------
+// Direct projector
+// ---------------------------------------------------------------------------
+template <int GEOM>
+__global__ void __launch_bounds__(512)
+k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
+                  const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
+                  long sino_view_stride, int band_rows, int *__restrict__ err)
+{
+  extern __shared__ float sm[];
+  __shared__ View3D sV;
+  __shared__ int s_next;
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nu = P.nu, nv = P.nv, nz = P.nz;
+  float *acc = sm;
+  float *prof = sm + band_rows * nu + warp * nu;
+  float *wv = sm + band_rows * nu + nwarps * nu + warp * band_rows;
+  const int vi = blockIdx.y;
+  if (threadIdx.x < (int)(sizeof(View3D) / 8))
+    reinterpret_cast<double *>(&sV)[threadIdx.x] =
+        reinterpret_cast<const double *>(views + vi)[threadIdx.x];
+  if (threadIdx.x == 0) s_next = 0;
+  const int v0 = blockIdx.x * band_rows;
+  const int v1 = min(v0 + band_rows, nv);
+  for (int t = threadIdx.x; t < band_rows * nu; t += blockDim.x) acc[t] = 0.f;
+  for (int t = lane; t < nu; t += 32) prof[t] = 0.f;
+  __syncthreads();
+  const View3D &V = sV;
+  const int ncols = P.nx * P.ny;
+  const int nchunks = (ncols + 31) >> 5;
+
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(&s_next, 1);
+    chunk = __shfl_sync(FULLM, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int mycol = (chunk << 5) + lane;
+    ColGeo<MODEL_CUBIC> c;
+    bool hit = false;
+    if (mycol < ncols) {
+      column_geo<GEOM, MODEL_CUBIC>(P, V, mycol % P.nx, mycol / P.nx, 0, c);
+      if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+      hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
+    }
+    unsigned mask = __ballot_sync(FULLM, hit);
+    while (mask) {
+      const int src = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const ColGeo<MODEL_CUBIC> cc = shfl_colc(c, src);
+      const int col = (chunk << 5) + src;
+      const int vl = cc.vax.lo, vr = cc.vax.lo + cc.vax.n;
+      const int rb = max(vl, v0), re = min(vr, v1), nr = re - rb;
+      for (int r = lane; r < nr; r += 32) wv[r] = axis_weight<MODEL_CUBIC>(cc.vax, rb - vl + r, P);
+      int lo = INT_MAX, hi = INT_MIN;
+      const long cbase = (long)col * nz;
+      for (int k0 = lane; k0 < nz; k0 += 64) {
+        const int k1 = k0 + 32;
+        const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
+        const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+        if (x0 == 0.0f && x1 == 0.0f) continue;
+        UPair up;
+        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+        if (x0 == 0.0f) up.n0 = 0;
+        if (x1 == 0.0f) up.n1 = 0;
+        const int L = max(up.n0, up.n1);
+        if (L <= 0) continue;
+        const float2 xr = mul2(make_float2(x0, x1), up.rho);
+        float2 Fp = cubic_prim2(up.start);
+        float2 lf = f2(1.0f);
+        for (int l = 0; l < L; ++l) {
+          const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+          const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
+          if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
+          if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
+          Fp = F;
+          lf = add2(lf, f2(1.0f));
+        }
+        if (up.n0 > 0) {
+          lo = min(lo, up.lo0);
+          hi = max(hi, up.lo0 + up.n0);
+        }
+        if (up.n1 > 0) {
+          lo = min(lo, up.lo1);
+          hi = max(hi, up.lo1 + up.n1);
+        }
+      }
+      lo = __reduce_min_sync(FULLM, lo);
+      hi = __reduce_max_sync(FULLM, hi);
+      __syncwarp();
+      if (lo < hi) {
+        for (int r = 0; r < nr; ++r) {
+          const float w = wv[r];
+          float *row = acc + (rb - v0 + r) * nu;
+          for (int u = lo + lane; u < hi; u += 32) atomicAdd(row + u, w * prof[u]);
+        }
+        __syncwarp();
+        for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  float *out = sino + (long)vi * sino_view_stride;
+  const int nrow = v1 - v0;
+  for (int t = threadIdx.x; t < nrow * nu; t += blockDim.x) {
+    const int r = t / nu, u = t - r * nu;
+    out[(long)(v0 + r) * nu + u] += acc[t];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Direct projector, atomic-free band accumulation ("pull").
+//
+// A CTA owns 32 detector rows of one view; each of its 16 warps owns two of
+// them (warp w: rows w and w+16) and each lane UC consecutive cells of both
+// rows, accumulated in registers.  Work proceeds in batches: every warp takes
+// its next column that touches the band, builds the column's u-profile
+// P[u] (sum over the column's voxels of rho * x * u-weight) in its shared
+// row and publishes the column's weights on the 32 band rows; after a
+// barrier every thread adds w(row) * P[u] of the 16 profiles into the cells
+// it owns.  Each detector cell has one owner, so no atomics are needed
+// outside the per-warp profiles and the summation order is fixed.
+// ---------------------------------------------------------------------------
+template <int GEOM, int UC>
+__global__ void __launch_bounds__(512, 1)
+k_fwd3d_pull(const Params3D P, const View3D *__restrict__ views,
+             const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
+             long sino_view_stride, int *__restrict__ err)
+{
+  constexpr int NW = 16, BR = 32, ROW = 32 * UC;
+  extern __shared__ float sm[];
+  float *prof_all = sm;               // NW rows of ROW floats
+  float *Wb = sm + NW * ROW;          // Wb[c * BR + r]: weight of warp c's column on band row r
+  int *rng = reinterpret_cast<int *>(Wb + NW * BR);  // [lo, hi) of each warp's profile
+  __shared__ View3D sV;
+  __shared__ int s_next;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nu = P.nu, nv = P.nv, nz = P.nz;
+  float *prof = prof_all + warp * ROW;
+  const int vi = blockIdx.y;
+  if (threadIdx.x < (int)(sizeof(View3D) / 8))
+    reinterpret_cast<double *>(&sV)[threadIdx.x] =
+        reinterpret_cast<const double *>(views + vi)[threadIdx.x];
+  if (threadIdx.x == 0) s_next = 0;
+  const int v0 = blockIdx.x * BR;
+  const int v1 = min(v0 + BR, nv);
+  for (int t = lane; t < ROW; t += 32) prof[t] = 0.f;
+  __syncthreads();
+  const View3D &V = sV;
+  const int ncols = P.nx * P.ny;
+  const int nchunks = (ncols + 31) >> 5;
+  float acc0[UC], acc1[UC];
+#pragma unroll
+  for (int q = 0; q < UC; ++q) {
+    acc0[q] = 0.f;
+    acc1[q] = 0.f;
+  }
+  // per-warp cursor over 32-column candidate chunks
+  unsigned mask = 0;
+  int chunk = -1;
+  bool exhausted = false;
+  ColGeo<MODEL_CUBIC> c;
+  c.vax.n = 0;
+  for (;;) {
+    int col = -1;
+    ColGeo<MODEL_CUBIC> cc;
+    while (!exhausted) {
+      if (mask == 0) {
+        int ch = 0;
+        if (lane == 0) ch = atomicAdd(&s_next, 1);
+        chunk = __shfl_sync(FULLM, ch, 0);
+        if (chunk >= nchunks) {
+          exhausted = true;
+          break;
+        }
+        const int mycol = (chunk << 5) + lane;
+        bool hit = false;
+        if (mycol < ncols) {
+          column_geo<GEOM, MODEL_CUBIC>(P, V, mycol % P.nx, mycol / P.nx, 0, c);
+          if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+          hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
+        }
+        mask = __ballot_sync(FULLM, hit);
+        continue;
+      }
+      const int src = __ffs(mask) - 1;
+      mask &= mask - 1;
+      cc = shfl_colc(c, src);
+      col = (chunk << 5) + src;
+      break;
+    }
+    const bool have = col >= 0;
+    int lo = INT_MAX, hi = INT_MIN;
+    // band weights of this warp's column (0 outside its footprint)
+    {
+      float w = 0.f;
+      const int r = v0 + lane;
+      if (have && lane < BR && r < v1 && r >= cc.vax.lo && r < cc.vax.lo + cc.vax.n)
+        w = axis_weight<MODEL_CUBIC>(cc.vax, r - cc.vax.lo, P);
+      if (lane < BR) Wb[warp * BR + lane] = w;
+    }
+    if (have) {
+      const long cbase = (long)col * nz;
+      for (int k0 = lane; k0 < nz; k0 += 64) {
+        const int k1 = k0 + 32;
+        const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
+        const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+        if (x0 == 0.0f && x1 == 0.0f) continue;
+        UPair up;
+        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+        if (x0 == 0.0f) up.n0 = 0;
+        if (x1 == 0.0f) up.n1 = 0;
+        const int L = max(up.n0, up.n1);
+        if (L <= 0) continue;
+        const float2 xr = mul2(make_float2(x0, x1), up.rho);
+        float2 Fp = cubic_prim2(up.start);
+        float2 lf = f2(1.0f);
+        for (int l = 0; l < L; ++l) {
+          const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+          const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
+          if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
+          if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
+          Fp = F;
+          lf = add2(lf, f2(1.0f));
+        }
+        if (up.n0 > 0) {
+          lo = min(lo, up.lo0);
+          hi = max(hi, up.lo0 + up.n0);
+        }
+        if (up.n1 > 0) {
+          lo = min(lo, up.lo1);
+          hi = max(hi, up.lo1 + up.n1);
+        }
+      }
+      lo = __reduce_min_sync(FULLM, lo);
+      hi = __reduce_max_sync(FULLM, hi);
+    }
+    if (lane == 0) {
+      rng[2 * warp] = lo;
+      rng[2 * warp + 1] = hi;
+    }
+    if (!__syncthreads_or(have ? 1 : 0)) break;
+    // pull: cells (row warp, row warp+16) x [ub, ub+UC)
+    const int ub = lane * UC;
+#pragma unroll 1
+    for (int cw = 0; cw < NW; ++cw) {
+      const float w0 = Wb[cw * BR + warp];
+      const float w1 = Wb[cw * BR + warp + NW];
+      if (w0 == 0.f && w1 == 0.f) continue;
+      const int clo = rng[2 * cw], chi = rng[2 * cw + 1];
+      if (ub + UC <= clo || ub >= chi) continue;
+      const float4 *pc = reinterpret_cast<const float4 *>(prof_all + cw * ROW + ub);
+#pragma unroll
+      for (int q = 0; q < UC / 4; ++q) {
+        const float4 p4 = pc[q];
+        acc0[4 * q + 0] = fmaf(w0, p4.x, acc0[4 * q + 0]);
+        acc0[4 * q + 1] = fmaf(w0, p4.y, acc0[4 * q + 1]);
+        acc0[4 * q + 2] = fmaf(w0, p4.z, acc0[4 * q + 2]);
+        acc0[4 * q + 3] = fmaf(w0, p4.w, acc0[4 * q + 3]);
+        acc1[4 * q + 0] = fmaf(w1, p4.x, acc1[4 * q + 0]);
+        acc1[4 * q + 1] = fmaf(w1, p4.y, acc1[4 * q + 1]);
+        acc1[4 * q + 2] = fmaf(w1, p4.z, acc1[4 * q + 2]);
+        acc1[4 * q + 3] = fmaf(w1, p4.w, acc1[4 * q + 3]);
+      }
+    }
+    __syncthreads();
+    if (have && lo < hi)
+      for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;
+    __syncwarp();
+  }
+  // write the owned cells back (each cell has exactly one owner)
+  float *out = sino + (long)vi * sino_view_stride;
+  const int ub = lane * UC;
+  const int r0 = v0 + warp, r1 = v0 + warp + NW;
+#pragma unroll
+  for (int q = 0; q < UC; ++q) {
+    const int u = ub + q;
+    if (u < nu) {
+      if (r0 < v1) out[(long)r0 * nu + u] += acc0[q];
+      if (r1 < v1) out[(long)r1 * nu + u] += acc1[q];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Transpose
+// ---------------------------------------------------------------------------
+template <int GEOM, int KP>
+__global__ void __launch_bounds__(256)
+k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
+                  const int *__restrict__ gate_ptr, const GateEntry *__restrict__ entries,
+                  int view_lo, int view_hi, const float *__restrict__ sino,
+                  long sino_view_stride, float *__restrict__ vol, long gate_stride,
+                  int *__restrict__ err)
+{
+  extern __shared__ float sm[];
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nu = P.nu, nz = P.nz;
+  const int ncols = P.nx * P.ny;
+  const int col = blockIdx.x * nwarps + warp;
+  if (col >= ncols) return;
+  float *Q = sm + warp * nu;
+  float *wv = sm + nwarps * nu + warp * 64;
+  const int i = col % P.nx, j = col / P.nx;
+  const int kbase = blockIdx.y * (64 * KP);
+  const int gate = blockIdx.z;
+  const int e0 = gate_ptr[gate], e1 = gate_ptr[gate + 1];
+  float2 acc[KP], cmp[KP];
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    acc[p] = f2(0.f);
+    cmp[p] = f2(0.f);
+  }
+
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int me = eb + lane;
+    ColGeo<MODEL_CUBIC> mine;
+    int myview = 0;
+    float myw = 0.f;
+    const GateEntry ge = (me < e1) ? entries[me] : GateEntry{-1, 0.f};
+    if (ge.view >= view_lo && ge.view < view_hi) {
+      myview = ge.view;
+      myw = ge.w;
+      column_geo<GEOM, MODEL_CUBIC>(P, views[myview], i, j, 0, mine);
+      if (mine.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+    } else {
+      mine.vax.n = 0;
+      mine.bad = 1;
+    }
+    const int cnt = min(32, e1 - eb);
+    for (int s = 0; s < cnt; ++s) {
+      const int nvx = __shfl_sync(FULLM, mine.vax.n, s);
+      const int bd = __shfl_sync(FULLM, mine.bad, s);
+      if (bd || nvx <= 0) continue;
+      const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
+      const int view = __shfl_sync(FULLM, myview, s);
+      const float wgt = __shfl_sync(FULLM, myw, s);
+      const View3D &V = views[view];
+      UPair up[KP];
+      int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
+        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up[p]);
+        if (k0 >= nz) up[p].n0 = 0;
+        if (k1 >= nz) up[p].n1 = 0;
+        if (up[p].n0 > 0) {
+          lo = min(lo, up[p].lo0);
+          hi = max(hi, up[p].lo0 + up[p].n0);
+        }
+        if (up[p].n1 > 0) {
+          lo = min(lo, up[p].lo1);
+          hi = max(hi, up[p].lo1 + up[p].n1);
+        }
+      }
+      lo = __reduce_min_sync(FULLM, lo);
+      hi = __reduce_max_sync(FULLM, hi);
+      if (lo >= hi) continue;
+      // v-collapsed profile Q[u] = sum_v wv(v) pix[v][u], u in [lo, hi).
+      // Each lane keeps up to QC cells of Q in registers (u = lo + lane + 32c)
+      // and walks the footprint rows; the QC loads of a row are independent,
+      // so a warp keeps many loads in flight.
+      const int npv = cc.vax.n;
+      const float *img0 = sino + (long)(view - view_lo) * sino_view_stride;
+      constexpr int QC = 16;
+      for (int ub = lo; ub < hi; ub += 32 * QC) {
+        float q[QC];
+#pragma unroll
+        for (int c = 0; c < QC; ++c) q[c] = 0.f;
+        for (int m0 = 0; m0 < npv; m0 += 32) {
+          const int mn = min(32, npv - m0);
+          const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+          for (int m = 0; m < mn; ++m) {
+            const float w = __shfl_sync(FULLM, wl, m);
+            const float *row = img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + lane;
+            float a[QC];
+#pragma unroll
+            for (int c = 0; c < QC; ++c) a[c] = (ub + lane + 32 * c < hi) ? __ldg(row + 32 * c) : 0.f;
+#pragma unroll
+            for (int c = 0; c < QC; ++c) q[c] = fmaf(w, a[c], q[c]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < QC; ++c)
+          if (ub + lane + 32 * c < hi) Q[ub + lane + 32 * c] = q[c];
+      }
+      __syncwarp();
+      // per-voxel gathers, two voxels per instruction
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        const int L = max(up[p].n0, up[p].n1);
+        if (L <= 0) continue;
+        float2 Fp = cubic_prim2(up[p].start);
+        float2 S = f2(0.f);
+        float2 lf = f2(1.0f);
+        for (int l = 0; l < L; ++l) {
+          const float2 F = cubic_prim2(fma2(lf, up[p].inc, up[p].start));
+          const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+          const float q0 = (l < up[p].n0) ? Q[up[p].lo0 + l] : 0.0f;
+          const float q1 = (l < up[p].n1) ? Q[up[p].lo1 + l] : 0.0f;
+          S = fma2(w, make_float2(q0, q1), S);
+          Fp = F;
+          lf = add2(lf, f2(1.0f));
+        }
+        // Kahan (packed): acc += wgt * rho * S
+        const float2 term = mul2(mul2(up[p].rho, S), f2(wgt));
+        const float2 y = add2(term, make_float2(-cmp[p].x, -cmp[p].y));
+        const float2 t = add2(acc[p], y);
+        cmp[p] = add2(add2(t, make_float2(-acc[p].x, -acc[p].y)), make_float2(-y.x, -y.y));
+        acc[p] = t;
+      }
+      __syncwarp();
+    }
+  }
+  float *dst = vol + (long)gate * gate_stride + (long)col * nz;
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
+    if (k0 < nz) dst[k0] += acc[p].x - cmp[p].x;
+    if (k1 < nz) dst[k1] += acc[p].y - cmp[p].y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers (cubic model, factorised views)
+// ---------------------------------------------------------------------------
+template <int GEOM, int UC>
+static cudaError_t fwd_pull(const Fwd3DLaunch &L, cudaStream_t st)
+{
+  dim3 grid((L.P.nv + 31) / 32, L.nviews);
+  const size_t smem = sizeof(float) * (16 * 32 * UC + 16 * 32) + sizeof(int) * 32;
+  auto kern = k_fwd3d_pull<GEOM, UC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 512, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino, L.sino_view_stride,
+                                L.err);
+  return cudaGetLastError();
+}
+
+template <int GEOM>
+static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
+{
+  if (L.pull) {
+    if (L.P.nu <= 128) return fwd_pull<GEOM, 4>(L, st);
+    if (L.P.nu <= 256) return fwd_pull<GEOM, 8>(L, st);
+    if (L.P.nu <= 512) return fwd_pull<GEOM, 16>(L, st);
+  }
+  dim3 grid((L.P.nv + L.band_rows - 1) / L.band_rows, L.nviews);
+  const size_t smem = sizeof(float) * ((size_t)L.band_rows * L.P.nu + (size_t)L.warps * L.P.nu +
+                                       (size_t)L.warps * L.band_rows);
+  auto kern = k_fwd3d_band_fast<GEOM>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, L.warps * 32, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino,
+                                        L.sino_view_stride, L.band_rows, L.err);
+  return cudaGetLastError();
+}
+
+template <int GEOM>
+static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
+{
+  constexpr int KP = 4;  // 4 voxel pairs per lane: 256 voxels per warp-column pass
+  const int warps = 8;
+  const int ncols = L.P.nx * L.P.ny;
+  dim3 grid((ncols + warps - 1) / warps, (L.P.nz + 64 * KP - 1) / (64 * KP), L.ngates);
+  const size_t smem = sizeof(float) * ((size_t)warps * L.P.nu + (size_t)warps * 64);
+  auto kern = k_back3d_col_fast<GEOM, KP>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, warps * 32, smem, st>>>(L.P, L.views, L.gate_ptr, L.entries, L.view_lo, L.view_hi,
+                                      L.sino, L.sino_view_stride, L.vol, L.gate_stride, L.err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
+{
+  return L.P.geom == GEOM_CONE ? fwd_fast<GEOM_CONE>(L, st) : fwd_fast<GEOM_PARALLEL>(L, st);
+}
+
+cudaError_t launch_back3d_fast(const Back3DLaunch &L, cudaStream_t st)
+{
+  return L.P.geom == GEOM_CONE ? back_fast<GEOM_CONE>(L, st) : back_fast<GEOM_PARALLEL>(L, st);
+}
+
+}  // namespace trtt

@@ -17,19 +17,23 @@ import numpy as np
 
 
 def ellipses_2d(nx: int, ny: int, n: int = 10, seed: int = 0,
-                dtype=np.float64) -> np.ndarray:
-    """``n`` random ellipses inside the inscribed disc, intensities U[0,1]."""
+                dtype=np.float64, body: bool = True) -> np.ndarray:
+    """``n`` random ellipses, intensities U[0,1]; the first is a large
+    centred "body" ellipse unless ``body=False``."""
     rng = np.random.default_rng(seed)
     y, x = np.mgrid[0:ny, 0:nx].astype(np.float64)
     x = (x - 0.5 * (nx - 1)) / (0.5 * nx)
     y = (y - 0.5 * (ny - 1)) / (0.5 * ny)
     img = np.zeros((ny, nx))
-    for _ in range(n):
+    for e in range(n):
         r = 0.6 * math.sqrt(rng.uniform())
         phi = rng.uniform(0, 2 * math.pi)
         cx, cy = r * math.cos(phi), r * math.sin(phi)
         a = rng.uniform(0.05, 0.35)
         b = rng.uniform(0.05, 0.35)
+        if body and e == 0:
+            cx = cy = 0.0
+            a, b = rng.uniform(0.85, 0.95, size=2)
         ang = rng.uniform(0, math.pi)
         val = rng.uniform(0.0, 1.0)
         ca, sa = math.cos(ang), math.sin(ang)
@@ -40,21 +44,30 @@ def ellipses_2d(nx: int, ny: int, n: int = 10, seed: int = 0,
 
 
 def ellipsoids_3d(nx: int, ny: int, nz: int, n: int = 20, seed: int = 0,
-                  dtype=np.float32, z_shift: float = 0.0) -> np.ndarray:
-    """``n`` random ellipsoids inside the inscribed cylinder, intensities
-    U[0,1].  ``z_shift`` translates every ellipsoid along z (in units of the
-    half height), as the 4D breathing phantom does between gates."""
+                  dtype=np.float32, z_shift: float = 0.0, body: bool = True) -> np.ndarray:
+    """``n`` random ellipsoids, intensities U[0,1].  As in the reference's
+    Shepp-Logan style generator, the first one is a large "body" ellipsoid
+    (transaxial semi-axes 0.85-0.95 of the half extent, longer than the
+    volume along z, centred) that the others sit in, so the volume is dense
+    like a patient scan (about 60% non-zero voxels); ``body=False`` draws only
+    small ellipsoids.  ``z_shift`` translates every ellipsoid along z (in
+    units of the half height), as the 4D breathing phantom does between
+    gates."""
     rng = np.random.default_rng(seed)
     vol = np.zeros((nz, ny, nx), dtype=np.float64)
     zz = (np.arange(nz) - 0.5 * (nz - 1)) / (0.5 * nz)
     yy = (np.arange(ny) - 0.5 * (ny - 1)) / (0.5 * ny)
     xx = (np.arange(nx) - 0.5 * (nx - 1)) / (0.5 * nx)
-    for _ in range(n):
+    for e in range(n):
         r = 0.55 * math.sqrt(rng.uniform())
         phi = rng.uniform(0, 2 * math.pi)
         cx, cy = r * math.cos(phi), r * math.sin(phi)
         cz = rng.uniform(-0.5, 0.5) + z_shift
         ax, ay, az = rng.uniform(0.06, 0.3, size=3)
+        if body and e == 0:
+            cx, cy, cz = 0.0, 0.0, z_shift
+            ax, ay = rng.uniform(0.85, 0.95, size=2)
+            az = rng.uniform(1.1, 1.3)
         ang = rng.uniform(0, math.pi)
         val = rng.uniform(0.0, 1.0)
         ca, sa = math.cos(ang), math.sin(ang)
