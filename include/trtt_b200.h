@@ -247,6 +247,25 @@ int trtt_b200_cb3d_batch(double *out, const double *in, long nx, long ny,
                          long nviews, const double *xos, const double *xsd,
                          int geometry, int job);
 
+/* Reconstruction helpers (device pointers, FP32 data, FP64 scalars).  The
+ * FP64 results are ADDED into *f_dev / *out_dev (device scalars), so several
+ * terms can be summed before one read-back.
+ * wls_residual: wr = w*(hx - y) (w may be NULL: unit weights) and
+ *   f += 1/2 sum w (hx - y)^2, the data term of Tomography_3D/Ytrtt3D_optim.i:186-201.
+ * dot: out += sum a*b accumulated in FP64.
+ * tv: isotropic smoothed total variation of z ([nz][ny][nx], nz = 1 in 2D),
+ *   f += mu * sum (sqrt(|grad z|^2 + eps^2) - eps), g += mu * dTV/dz.
+ * spline_sample: z = S x, the cubic B-spline coefficients x sampled at the
+ *   voxel centres (separable [1/6, 2/3, 1/6], zero outside); S is symmetric
+ *   so the same call applies S^T.  tmp: scratch of the same size. */
+int trtt_b200_wls_residual(const float *hx, const float *y, const float *w, float *wr, long n,
+                           double *f_dev, void *stream);
+int trtt_b200_dot(const float *a, const float *b, long n, double *out_dev, void *stream);
+int trtt_b200_tv(const float *z, long nx, long ny, long nz, double eps, double mu, float *g,
+                 double *f_dev, void *stream);
+int trtt_b200_spline_sample(const float *x, float *z, float *tmp, long nx, long ny, long nz,
+                            void *stream);
+
 /* Allocation-free cone-beam direct projector.  No counterpart in the
  * reference (whose plugin allocates on the host per voxel).  For callers that
  * cannot call cudaMalloc: code running while a stream is captured into a

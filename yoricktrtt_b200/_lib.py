@@ -65,6 +65,10 @@ SIGNATURES = {
     "trtt_b200_plan2d_destroy": (_I, [_vp]),
     "trtt_b200_cb3d_cubic_forward_noalloc": (_I, [_vp, _vp, _L, _L, _L, _D, _I, _L, _L, _D, _D,
                                                    _L, _dp, _dp, _vp]),
+    "trtt_b200_wls_residual": (_I, [_vp, _vp, _vp, _vp, _L, _vp, _vp]),
+    "trtt_b200_dot": (_I, [_vp, _vp, _L, _vp, _vp]),
+    "trtt_b200_tv": (_I, [_vp, _L, _L, _L, _D, _D, _vp, _vp, _vp]),
+    "trtt_b200_spline_sample": (_I, [_vp, _vp, _vp, _L, _L, _L, _vp]),
     "trtt_b200_cb3d_batch": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
                                    _D, _L, _dp, _dp, _I, _I]),
 }

@@ -1,0 +1,306 @@
+"""Regularised reconstruction on the GPU: weighted least squares + total
+variation, minimised by VMLM-B (limited-memory variable metric with bound
+constraints).
+
+Mirrors the cost function of the reference
+(``Tomography_3D/Ytrtt3D_optim.i:128-234``):
+
+    f(x) = 1/2 sum_k (H_k x - y_k)' W_k (H_k x - y_k) + mu * TV(S x)
+
+with x the B-spline coefficients, S the sampling of the spline at the voxel
+centres and TV the smoothed isotropic total variation, minimised under the
+bounds ``lower <= x <= upper`` by ``op_mnb`` (OptimPack's VMLM-B, called at
+``Tomography_3D/Ytrtt3D_optim.i:663``).  OptimPack and YTotVar are external
+packages absent from the reference repository, so the optimiser and the
+regulariser here are restated from their published definitions
+(Thiebaut 2002, "Optimization issues in blind deconvolution algorithms";
+smoothed TV sqrt(|grad z|^2 + eps^2)); ``oracle/recon_oracle.py`` is the FP64
+CPU restatement of the same iteration used to check this one.
+
+All vectors stay on the device in FP32; inner products, the objective and
+the line-search scalars are FP64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class _Scalar:
+    """A device FP64 accumulator read back after each kernel sequence."""
+
+    def __init__(self, device):
+        torch = _torch()
+        self.t = torch.zeros(1, dtype=torch.float64, device=device)
+
+    def reset(self):
+        self.t.zero_()
+        return _ptr(self.t)
+
+    def value(self) -> float:
+        return float(self.t.item())
+
+
+def dot(a, b, acc: _Scalar | None = None) -> float:
+    """FP64-accumulated inner product of two FP32 device tensors."""
+    acc = acc or _Scalar(a.device)
+    _lib.check(_lib.load().trtt_b200_dot(_ptr(a), _ptr(b), a.numel(), acc.reset(), _stream()),
+               "trtt_b200_dot")
+    return acc.value()
+
+
+class Projector2D:
+    """All views of a 2D B-spline (trtt_PB2D/FB2D) or Long-Fessler scan on
+    one GPU.  Images are (ny, nx) float32, sinograms (nviews, nv)."""
+
+    def __init__(self, scan=None, table=None, lf_params=None, beta=None, offset=None,
+                 line_integ=False):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise _lib.TrttError("Projector2D needs a CUDA device (no CPU fallback)")
+        lib = _lib.load()
+        h = C.c_void_p()
+        if lf_params is not None:
+            beta = np.ascontiguousarray(beta, dtype=np.float64)
+            offset = np.ascontiguousarray(offset, dtype=np.float64)
+            rc = lib.trtt_b200_plan2d_create_lf(C.byref(h), C.addressof(lf_params),
+                                                1 if line_integ else 0, len(beta),
+                                                _lib.dptr(beta), _lib.dptr(offset))
+            self.nx, self.ny = lf_params.objectDimension1, lf_params.objectDimension2
+            self.nv, self.nviews = lf_params.detectorDimension, len(beta)
+        else:
+            from .geometry import TRTT_PARALLEL_BEAM
+            geom = 3 if scan.mode == TRTT_PARALLEL_BEAM else 5
+            xos = np.ascontiguousarray(scan.xos)
+            xsd = np.ascontiguousarray(scan.xsd)
+            if table is None:
+                rc = lib.trtt_b200_plan2d_create(C.byref(h), geom, scan.nx, scan.ny, scan.s_scl,
+                                                 scan.s_deg, None, 0, 1.0, None, scan.nv,
+                                                 scan.v_scl, scan.nviews, _lib.dptr(xos),
+                                                 _lib.dptr(xsd))
+            else:
+                rc = lib.trtt_b200_plan2d_create(C.byref(h), geom, scan.nx, scan.ny, scan.s_scl,
+                                                 scan.s_deg, _lib.dptr(table.cum), table.size,
+                                                 table.step, _lib.dptr(table.coord), scan.nv,
+                                                 scan.v_scl, scan.nviews, _lib.dptr(xos),
+                                                 _lib.dptr(xsd))
+            self.nx, self.ny, self.nv, self.nviews = scan.nx, scan.ny, scan.nv, scan.nviews
+        _lib.check(rc, "trtt_b200_plan2d_create")
+        self._h = h
+
+    def forward(self, x, out=None):
+        torch = _torch()
+        if out is None:
+            out = torch.zeros(self.nviews, self.nv, dtype=torch.float32, device=x.device)
+        _lib.check(_lib.load().trtt_b200_plan2d_forward(self._h, _ptr(x), _ptr(out), _stream()),
+                   "trtt_b200_plan2d_forward")
+        return out
+
+    def backward(self, y, out=None):
+        torch = _torch()
+        if out is None:
+            out = torch.zeros(self.ny, self.nx, dtype=torch.float32, device=y.device)
+        _lib.check(_lib.load().trtt_b200_plan2d_backward(self._h, _ptr(y), _ptr(out), _stream()),
+                   "trtt_b200_plan2d_backward")
+        return out
+
+    def status(self):
+        _lib.check(_lib.load().trtt_b200_plan2d_status(self._h, _stream()), "projector")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().trtt_b200_plan2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Objective:
+    """f(x) = 1/2 ||Hx - y||^2_W + mu TV(S x) and its gradient.
+
+    ``proj`` has forward(x, out) / backward(r, out) (Projector2D, or
+    Projector3D on (nz, ny, nx) volumes); ``y`` and ``w`` have the detector
+    shape (``w`` None: unit weights).  ``spline=True`` applies TV to the
+    spline samples S x, as the reference does; False to x itself."""
+
+    def __init__(self, proj, y, w=None, mu=0.0, eps=1e-3, spline=True):
+        torch = _torch()
+        self.proj, self.y, self.w = proj, y, w
+        self.mu, self.eps, self.spline = float(mu), float(eps), spline
+        self.hx = torch.empty_like(y)
+        self.wr = torch.empty_like(y)
+        self._acc = _Scalar(y.device)
+        self.nevals = 0
+
+    def _dims(self, x):
+        if x.dim() == 2:
+            return x.shape[1], x.shape[0], 1
+        return x.shape[2], x.shape[1], x.shape[0]
+
+    def __call__(self, x):
+        torch = _torch()
+        lib = _lib.load()
+        st = _stream()
+        self.hx.zero_()
+        self.proj.forward(x, out=self.hx)
+        facc = self._acc.reset()
+        _lib.check(lib.trtt_b200_wls_residual(_ptr(self.hx), _ptr(self.y),
+                                              _ptr(self.w) if self.w is not None else None,
+                                              _ptr(self.wr), self.y.numel(), facc, st),
+                   "trtt_b200_wls_residual")
+        g = torch.zeros_like(x)
+        self.proj.backward(self.wr, out=g)
+        if self.mu > 0:
+            nx, ny, nz = self._dims(x)
+            if self.spline:
+                z = torch.empty_like(x)
+                tmp = torch.empty_like(x)
+                _lib.check(lib.trtt_b200_spline_sample(_ptr(x), _ptr(z), _ptr(tmp), nx, ny, nz, st),
+                           "spline_sample")
+                gz = torch.zeros_like(x)
+                _lib.check(lib.trtt_b200_tv(_ptr(z), nx, ny, nz, self.eps, self.mu, _ptr(gz),
+                                            facc, st), "trtt_b200_tv")
+                sg = torch.empty_like(x)
+                _lib.check(lib.trtt_b200_spline_sample(_ptr(gz), _ptr(sg), _ptr(tmp), nx, ny, nz, st),
+                           "spline_sample")
+                g += sg
+            else:
+                _lib.check(lib.trtt_b200_tv(_ptr(x), nx, ny, nz, self.eps, self.mu, _ptr(g), facc, st),
+                           "trtt_b200_tv")
+        self.nevals += 1
+        return self._acc.value(), g
+
+
+@dataclass
+class VMLMBInfo:
+    iterations: int = 0
+    evaluations: int = 0
+    f: list = field(default_factory=list)
+    times: list = field(default_factory=list)
+    converged: bool = False
+    reason: str = ""
+
+
+def vmlmb(fg, x0, lower=0.0, upper=None, mem=5, maxiter=100, frtol=1e-6, armijo=1e-4,
+          max_backtrack=30, callback=None):
+    """VMLM-B: L-BFGS restricted to the free variables of the box
+    lower <= x <= upper, projected Armijo backtracking with safeguarded
+    quadratic steps, stop when |f_k - f_{k+1}| <= frtol max(|f_k|,|f_{k+1}|).
+
+    The same rules are restated in FP64 on the CPU by oracle/recon_oracle.py.
+    Returns (x, VMLMBInfo)."""
+    torch = _torch()
+    lo = -math.inf if lower is None else float(lower)
+    hi = math.inf if upper is None else float(upper)
+    acc = _Scalar(x0.device)
+
+    def clip(v):
+        return v.clamp(min=None if lo == -math.inf else lo, max=None if hi == math.inf else hi)
+
+    def d64(a, b):
+        return dot(a, b, acc)
+
+    t0 = time.perf_counter()
+    x = clip(x0.clone())
+    f, g = fg(x)
+    info = VMLMBInfo(evaluations=1, f=[f], times=[0.0])
+    S, Y = [], []
+    for it in range(1, maxiter + 1):
+        free = torch.ones_like(x)
+        if lo > -math.inf:
+            free[(x <= lo) & (g > 0)] = 0.0
+        if hi < math.inf:
+            free[(x >= hi) & (g < 0)] = 0.0
+        pg = g * free
+        pgn = math.sqrt(d64(pg, pg))
+        if pgn == 0.0:
+            info.converged, info.reason = True, "projected gradient is zero"
+            break
+        # two-loop recursion on the free subspace
+        q = pg.clone()
+        used = []
+        for s, y in reversed(list(zip(S, Y))):
+            sf, yf = s * free, y * free
+            sy = d64(sf, yf)
+            if sy <= 0.0:
+                continue
+            a = d64(sf, q) / sy
+            q -= a * yf
+            used.append((sf, yf, sy, a))
+        if used:
+            sf, yf, sy, _ = used[0]
+            q *= sy / d64(yf, yf)
+            for sf, yf, sy, a in reversed(used):
+                b = d64(yf, q) / sy
+                q += (a - b) * sf
+            d = -(q * free)
+            alpha = 1.0
+        else:
+            d = -pg
+            xn = math.sqrt(d64(x, x))
+            alpha = (0.1 * xn if xn > 0 else 1.0) / pgn
+        gd = d64(g, d)
+        if gd >= 0.0:  # not a descent direction: restart with the gradient
+            S.clear()
+            Y.clear()
+            d = -pg
+            xn = math.sqrt(d64(x, x))
+            alpha = (0.1 * xn if xn > 0 else 1.0) / pgn
+            gd = d64(g, d)
+        for _ in range(max_backtrack):
+            xt = clip(x + alpha * d)
+            ft, gt = fg(xt)
+            info.evaluations += 1
+            step = xt - x
+            if ft <= f + armijo * d64(g, step):
+                break
+            # safeguarded quadratic interpolation of phi(alpha)
+            denom = 2.0 * (ft - f - gd * alpha)
+            aq = -gd * alpha * alpha / denom if denom > 0 else 0.5 * alpha
+            alpha = min(max(aq, 0.1 * alpha), 0.5 * alpha)
+        else:
+            info.reason = "line search failed"
+            break
+        s = xt - x
+        yv = gt - g
+        if d64(s, yv) > 0.0:
+            S.append(s)
+            Y.append(yv)
+            if len(S) > mem:
+                S.pop(0)
+                Y.pop(0)
+        fprev = f
+        x, f, g = xt, ft, gt
+        info.iterations = it
+        info.f.append(f)
+        info.times.append(time.perf_counter() - t0)
+        if callback:
+            callback(it, x, f)
+        if abs(fprev - f) <= frtol * max(abs(fprev), abs(f)):
+            info.converged, info.reason = True, "relative objective change below frtol"
+            break
+    return x, info
