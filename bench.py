@@ -383,11 +383,22 @@ def main(argv=None):
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--workload", default="pair3d",
+                    choices=["pair3d", "parallel2d_recon", "fan2d", "cone3d_recon", "gates4d"],
+                    help="pair3d (default) is the benchmark line; the others measure the "
+                         "remaining configurations (yoricktrtt_b200/workloads.py)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "pair3d":
+        import torch
+        from yoricktrtt_b200 import workloads
+        torch.cuda.set_device(_env_int("LOCAL_RANK", 0))
+        res = getattr(workloads, args.workload)()
+        print(json.dumps({"workload": args.workload, **res}))
+        return 0
     return run_b200(args)
 
 

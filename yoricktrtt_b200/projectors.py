@@ -16,6 +16,7 @@ axis.  Detector stacks are (nviews, nv, nu).  Results are accumulated into
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -149,6 +150,59 @@ class Projector3D:
         if job == 1:
             return self.backward(x, **kw)
         raise ValueError("unsupported job (0 = direct, 1 = transpose)")
+
+    # -- tuning and graph capture ----------------------------------------------
+    TILE_CANDIDATES = [(0, 0), (16, 16), (24, 16), (32, 8), (32, 12), (48, 8), (-2, 0)]
+
+    def autotune(self, vol=None, layout="columns", candidates=None, reps=2, nview=None):
+        """Time the direct projector with each candidate (band_rows, warps)
+        setting (see trtt_b200_plan3d_set_tiles; (-2, 0) is the atomic-free
+        band kernel) on `vol` (random data of the plan's volume shape if
+        None) and keep the fastest.  Returns {candidate: ms} and the choice."""
+        torch = _torch()
+        if vol is None:
+            vol = torch.rand(self.volume_shape(layout), device=self.device)
+        nview = min(self.scan.nviews, nview or 32)
+        out = torch.zeros(self.detector_shape(nview), device=vol.device)
+        times = {}
+        for cand in candidates or self.TILE_CANDIDATES:
+            try:
+                self.set_tiles(*cand)
+            except _lib.TrttError:
+                continue
+            self.forward(vol, out=out, nview=nview, layout=layout)
+            torch.cuda.synchronize()
+            best = math.inf
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                self.forward(vol, out=out, nview=nview, layout=layout)
+                b.record()
+                torch.cuda.synchronize()
+                best = min(best, a.elapsed_time(b))
+            times[cand] = best
+        choice = min(times, key=times.get)
+        self.set_tiles(*choice)
+        self.tiles = choice
+        return times, choice
+
+    def capture(self, fn):
+        """Capture `fn()` (a sequence of forward/backward calls on fixed
+        tensors) into a CUDA graph after one warm-up run; returns the graph
+        (replay with graph.replay())."""
+        torch = _torch()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            fn()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        torch.cuda.synchronize()
+        return g
 
     def status(self, stream=None) -> None:
         """Raise if a kernel flagged an error (a voxel in the source plane)."""

@@ -1,0 +1,216 @@
+"""Measured workloads for the benchmark configurations other than the
+cone-beam projector pair (which bench.py times by default).
+
+Each function builds the configuration with seeded synthetic data, runs it on
+the current CUDA device and returns a dict of measured quantities (CUDA-event
+or wall-clock times, errors against the FP64 oracle where one applies).
+
+* ``parallel2d_recon``: 2D parallel beam, 256^2 image of 10 ellipses, cubic
+  B-spline, 180 views over [0, pi), 367 bins, 1% Gaussian noise; one
+  projector pair plus 50 VMLM-B iterations with TV (mu = 1e-2).
+* ``fan2d``: 2D fan beam, 512^2 image, 720 views over 2 pi, 1024-bin flat
+  detector, SID 1000 mm, SDD 1500 mm, 0.5 mm pixels: B-spline (closed-form
+  and table footprints) and Long-Fessler pair throughput, parity against the
+  FP64 oracle on sample views, FP64 adjoint test.
+* ``cone3d_recon``: 3D cone beam 256^3 -> 360 x 512^2, VMLM-B + TV until the
+  relative objective change falls below 1e-6 (at most 100 iterations).
+* ``gates4d``: 10 respiratory gates of 128x128x64, ellipsoid phantom
+  translated along z by up to 10 mm, views per gate drawn from U{20..60},
+  256^2 detector; all gates projected (direct and transpose) by one launch
+  each, tiles autotuned, the pair captured in a CUDA graph and replayed.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _events():
+    torch = _torch()
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _time(fn, reps=3):
+    torch = _torch()
+    fn()
+    torch.cuda.synchronize()
+    best = math.inf
+    for _ in range(reps):
+        a, b = _events()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def parallel2d_recon(iterations=50, seed=0):
+    torch = _torch()
+    from . import geometry as G, phantoms as P
+    from .recon import Objective, Projector2D, vmlmb
+    sc = G.circular_scan_2d(256, 256, 1.0, 3, 367, 1.0, 180, mode=G.TRTT_PARALLEL_BEAM)
+    truth = P.ellipses_2d(256, 256, n=10, seed=seed)
+    pr = Projector2D(sc)
+    xt = torch.tensor(truth, dtype=torch.float32, device="cuda")
+    y = pr.forward(xt)
+    rng = np.random.default_rng(seed + 1)
+    noise = torch.tensor(rng.standard_normal(tuple(y.shape)), dtype=torch.float32, device="cuda")
+    y = y + 0.01 * float(y.max()) * noise
+    out_f = torch.zeros_like(y)
+    out_b = torch.zeros_like(xt)
+    t_pair = _time(lambda: (pr.forward(xt, out=out_f.zero_()), pr.backward(y, out=out_b.zero_())))
+    obj = Objective(pr, y, mu=1e-2, eps=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x, info = vmlmb(obj, torch.zeros_like(xt), lower=0.0, maxiter=iterations, frtol=0.0)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    pr.status()
+    err = float(torch.linalg.norm(x - xt) / torch.linalg.norm(xt))
+    return {"config": "2D parallel 256^2, 180 views, 367 bins, cubic, VMLM-B + TV mu=1e-2",
+            "pair_ms": t_pair, "iterations": info.iterations, "evaluations": info.evaluations,
+            "recon_s": wall, "f_first": info.f[0], "f_last": info.f[-1],
+            "rel_err_vs_phantom": err}
+
+
+def fan2d(sample_views=4, seed=0):
+    torch = _torch()
+    from oracle import oracle  # checker only
+    from . import dropin, footprint as F, geometry as G, phantoms as P
+    from .recon import Projector2D, dot
+    sc = G.circular_scan_2d(512, 512, 0.5, 3, 1024, 0.5, 720, mode=G.TRTT_FAN_BEAM,
+                            rsc=1000.0, rsd=1500.0)
+    img = P.ellipses_2d(512, 512, n=10, seed=seed)
+    xt = torch.tensor(img, dtype=torch.float32, device="cuda")
+    orc = oracle.get("port")
+    res = {"config": "2D fan 512^2, 720 views / 2 pi, 1024 bins, SID 1000, SDD 1500, 0.5 mm"}
+    tab = F.make_footprint(3, 10001)
+    views = np.linspace(0, 719, sample_views).astype(int)
+    for name, pr, ref_fn in [
+        ("bspline_cubic", Projector2D(sc), lambda v, out: orc.p2d("FB2D", out, img, sc, int(v), 0, None)),
+        ("bspline_table", Projector2D(sc, tab), lambda v, out: orc.p2d("FB2D", out, img, sc, int(v), 0, tab)),
+    ]:
+        y = torch.zeros(sc.nviews, sc.nv, device="cuda")
+        b = torch.zeros_like(xt)
+        tf = _time(lambda: pr.forward(xt, out=y.zero_()))
+        yy = torch.rand_like(y)
+        tb = _time(lambda: pr.backward(yy, out=b.zero_()))
+        pr.forward(xt, out=y.zero_())
+        yh = y.double().cpu().numpy()
+        errs = []
+        for v in views:
+            ref = np.zeros(sc.nv)
+            ref_fn(v, ref)
+            errs.append(float(np.linalg.norm(yh[v] - ref) / np.linalg.norm(ref)))
+        pr.backward(yy, out=b.zero_())
+        adj = abs(dot(y, yy) - dot(xt, b)) / (math.sqrt(dot(y, y)) * math.sqrt(dot(yy, yy)))
+        res[name] = {"fwd_ms": tf, "back_ms": tb, "projections_per_s": 2 * sc.nviews / ((tf + tb) / 1e3),
+                     "max_rel_l2_vs_fp64": max(errs), "adjoint_rel": adj}
+    # Long-Fessler with the same geometry (Ytrtt_2D_projectors_Long_Fessler.i:216-233)
+    lfp = dropin.LF2DParams(pixelSize=0.5, pixelStep=0.5, voxelSize=0.5, sourceDistance=1000.0,
+                            detectorDistance=500.0, objectOffset1=0.0, objectOffset2=0.0,
+                            objectDimension1=512, objectDimension2=512, detectorDimension=1024)
+    from oracle.oracle import LF2DParams as OP
+    olp = OP(pixelSize=0.5, pixelStep=0.5, voxelSize=0.5, sourceDistance=1000.0,
+             detectorDistance=500.0, objectOffset1=0.0, objectOffset2=0.0,
+             objectDimension1=512, objectDimension2=512, detectorDimension=1024)
+    beta = sc.theta - math.pi / 2
+    offs = np.zeros(sc.nviews)
+    pr = Projector2D(lf_params=lfp, beta=beta, offset=offs)
+    y = torch.zeros(sc.nviews, 1024, device="cuda")
+    b = torch.zeros_like(xt)
+    tf = _time(lambda: pr.forward(xt, out=y.zero_()))
+    yy = torch.rand_like(y)
+    tb = _time(lambda: pr.backward(yy, out=b.zero_()))
+    pr.forward(xt, out=y.zero_())
+    yh = y.double().cpu().numpy()
+    errs = []
+    for v in views:
+        ref = np.zeros(1024)
+        orc.lf2d("direct", olp, beta[v], 0.0, img, ref, 1)
+        errs.append(float(np.linalg.norm(yh[v] - ref) / np.linalg.norm(ref)))
+    pr.backward(yy, out=b.zero_())
+    adj = abs(dot(y, yy) - dot(xt, b)) / (math.sqrt(dot(y, y)) * math.sqrt(dot(yy, yy)))
+    res["long_fessler"] = {"fwd_ms": tf, "back_ms": tb,
+                           "projections_per_s": 2 * sc.nviews / ((tf + tb) / 1e3),
+                           "max_rel_l2_vs_fp64": max(errs), "adjoint_rel": adj}
+    return res
+
+
+def cone3d_recon(maxiter=100, frtol=1e-6, seed=0, n=256, nd=512, views=360):
+    torch = _torch()
+    from . import geometry as G, phantoms as P
+    from .projectors import Projector3D
+    from .recon import Objective, vmlmb
+    sc = G.circular_scan_3d(n, n, n, 1.0, 3, nd, nd, 1.0, 1.0, views)
+    truth = torch.tensor(P.ellipsoids_3d(n, n, n, n=20, seed=seed), device="cuda")
+    pr = Projector3D(sc)
+    y = pr.forward(truth)
+    rng = np.random.default_rng(seed + 1)
+    y = y + 0.01 * float(y.max()) * torch.tensor(rng.standard_normal(tuple(y.shape)),
+                                                 dtype=torch.float32, device="cuda")
+    obj = Objective(pr, y, mu=1e-2, eps=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x, info = vmlmb(obj, torch.zeros_like(truth), lower=0.0, maxiter=maxiter, frtol=frtol)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    pr.status()
+    err = float(torch.linalg.norm(x - truth) / torch.linalg.norm(truth))
+    return {"config": f"3D cone {n}^3 -> {views} x {nd}^2, VMLM-B + TV to {frtol:g} relative objective change",
+            "iterations": info.iterations, "evaluations": info.evaluations,
+            "converged": info.converged, "reason": info.reason, "time_to_tol_s": wall,
+            "f_first": info.f[0], "f_last": info.f[-1], "rel_err_vs_phantom": err}
+
+
+def gates4d(nt=10, seed=0, replays=5):
+    torch = _torch()
+    from . import geometry as G, phantoms as P
+    from .projectors import Projector3D
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(20, 61, nt)
+    # each gate's views sit at fractional gate indices inside [g, g+1)
+    t_index = np.concatenate([g + rng.uniform(0.0, 1.0, c) for g, c in enumerate(counts)])
+    nviews = int(counts.sum())
+    # acquisition order: angles over the orbit as the dates advance
+    theta = np.sort(rng.uniform(0, 2 * math.pi, nviews))
+    sc = G.circular_scan_3d(128, 128, 64, 1.0, 3, 256, 256, 1.0, 1.0, nviews, theta=theta)
+    gates = torch.tensor(P.breathing_gates(128, 128, 64, nt, 1.0, amplitude_mm=10.0, seed=seed),
+                         device="cuda")
+    pr = Projector3D(sc)
+    pr.set_gates(nt, t_index)
+    from .projectors import columns_from_xyz
+    xc = columns_from_xyz(gates)
+    times, choice = pr.autotune(xc, layout="columns", nview=nviews, reps=2)
+    y = torch.zeros(pr.detector_shape(), device="cuda")
+    back = torch.zeros_like(xc)
+
+    def pair():
+        y.zero_()
+        back.zero_()
+        pr.forward(xc, out=y, layout="columns")
+        pr.backward(y, out=back, layout="columns")
+
+    graph = pr.capture(pair)
+    torch.cuda.synchronize()
+    best = math.inf
+    for _ in range(replays):
+        a, b = _events()
+        a.record()
+        graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    pr.status()
+    return {"config": f"4D: {nt} gates of 128x128x64, views per gate U{{20..60}} (total {nviews}), 256^2",
+            "views_per_gate": counts.tolist(), "tiles": list(choice),
+            "autotune_ms": {str(k): v for k, v in times.items()},
+            "pair_graph_ms": best, "projections_per_s": 2 * nviews / (best / 1e3)}
