@@ -26,6 +26,8 @@
 #ifndef TRTT_B200_H
 #define TRTT_B200_H 1
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -289,6 +291,70 @@ int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, float *sino,
                                          double v_scl, long nviews,
                                          const double *xos, const double *xsd,
                                          void *stream);
+
+/* Learned warm start: building blocks of a 3D U-Net on the sm_100a tensor
+ * cores.  No counterpart in the reference (its reconstructions start from
+ * zero, Tomography_3D/Ytrtt3D_optim.i:663).  All arrays are device arrays.
+ *
+ * Activation layout: a batch of nb volumes of d x h x w voxels with C BF16
+ * channels is stored "padded channels-last": nb (d+2)(h+2)(w+2) rows of C
+ * values, row ((v (d+2) + z)(h+2) + y)(w+2) + x, interior z in 1..d, y in
+ * 1..h, x in 1..w.  The one-voxel border must be zero; no call writes it.
+ *
+ * conv3_pack: FP32 weights w[cout][27][cin] (tap = 9 (dz+1) + 3 (dy+1) +
+ *   (dx+1)) -> BF16 operand tiles.  transpose = 0: the forward operand
+ *   (27 * roundup16(cout) * cin values); transpose = 1: the input-gradient
+ *   operand (weights transposed and flipped, 27 * cin * roundup16(cout)).
+ *   cin must be a multiple of 16.
+ * conv3_forward: 3x3x3 convolution, zero padding, of the channels of x1
+ *   (c1) followed by those of x2 (c2; x2 may be NULL with c2 = 0), c1, c2
+ *   multiples of 16, into n output channels (multiple of 16, <= 256) with the
+ *   packed weights of conv3_pack.  mode 0: y = act(conv + bias) as BF16
+ *   [rows][n], act(v) = v > 0 ? v : slope v; mode 1: the same in FP32;
+ *   mode 2: y[p] = resid[p] + conv[p][0] + bias[0] (FP32, one channel;
+ *   resid and y padded FP32 [rows]); mode 3 (gradients): output channels
+ *   [0, n1) go to y ([rows][n1]) and [n1, n) to y2 ([rows][n - n1]), BF16,
+ *   added to the present values when accumulate != 0, no bias/activation.
+ * conv3_wgrad: dw[cout][27][cin] = sum over rows of dy[row][co] *
+ *   x[row + off(tap)][ci] (x = x1 channels then x2 channels), db[co] =
+ *   sum dy[row][co] (db may be NULL).  cout in {16, 32, 48, 64}, cin =
+ *   c1 + c2 a multiple of 16 with 3 cin <= 512.  scratch: device buffer of
+ *   at least conv3_wgrad_scratch() bytes.
+ * unet_resample: between a fine grid (d, h, w even) and the coarse grid
+ *   (d/2, h/2, w/2), C channels (multiple of 8): mode 0 coarse = mean of the
+ *   2x2x2 children, 1 children (+)= coarse / 8, 2 children = coarse (nearest
+ *   upsampling), 3 coarse (+)= sum of children; (+)= when accumulate != 0.
+ * unet_act_grad: g *= (y > 0 ? 1 : slope), rows x C BF16 values.
+ * unet_pad_input: dense FP32 x[nb][d][h][w] -> xb ([rows][16] BF16,
+ *   channel 0 = scale x) and xf ([rows] FP32 = scale x; may be NULL).
+ * unet_unpad: padded FP32 [rows] -> dense FP32 times scale.
+ * unet_mse: *loss += mean over voxels of (out - scale target)^2 (FP64) and,
+ *   if dout is not NULL, dout[row][0] = its derivative (BF16 [rows][16]).
+ * adam: Adam step number `step` (>= 1) with decoupled-free L2 term
+ *   weight_decay * w added to the gradient.
+ * unet_status: -1 if a convolution kernel gave up waiting for its tensor-core
+ *   work (bounded waits), then clears the flag; synchronises the stream. */
+int trtt_b200_conv3_pack(const float *w, int cout, int cin, int transpose, void *wpack, void *stream);
+int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, const void *wpack, int n,
+                            const float *bias, int mode, float slope, void *y, void *y2, int n1,
+                            int accumulate, const float *resid, int nb, int d, int h, int w,
+                            void *stream);
+size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w);
+int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2,
+                          float *dw, float *db, void *scratch, size_t scratch_bytes, int nb, int d,
+                          int h, int w, void *stream);
+int trtt_b200_unet_resample(void *fine, void *coarse, int c, int nb, int d, int h, int w, int mode,
+                            int accumulate, void *stream);
+int trtt_b200_unet_act_grad(void *g, const void *y, long rows, int c, float slope, void *stream);
+int trtt_b200_unet_pad_input(const float *x, void *xb, float *xf, float scale, int nb, int d, int h,
+                             int w, void *stream);
+int trtt_b200_unet_unpad(const float *xf, float *x, float scale, int nb, int d, int h, int w,
+                         void *stream);
+int trtt_b200_unet_mse(const float *out, const float *target, void *dout, float scale, double *loss,
+                       int nb, int d, int h, int w, void *stream);
+int trtt_b200_adam(float *w, const float *g, float *m, float *v, long n, float lr, float b1, float b2,
+                   float eps, int step, float weight_decay, void *stream);
+int trtt_b200_unet_status(void *stream);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,20 @@ SIGNATURES = {
     "trtt_b200_spline_sample": (_I, [_vp, _vp, _vp, _L, _L, _L, _vp]),
     "trtt_b200_cb3d_batch": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
                                    _D, _L, _dp, _dp, _I, _I]),
+    "trtt_b200_conv3_pack": (_I, [_vp, _I, _I, _I, _vp, _vp]),
+    "trtt_b200_conv3_forward": (_I, [_vp, _I, _vp, _I, _vp, _I, _vp, _I, C.c_float, _vp, _vp, _I,
+                                      _I, _vp, _I, _I, _I, _I, _vp]),
+    "trtt_b200_conv3_wgrad_scratch": (C.c_size_t, [_I, _I, _I, _I, _I, _I]),
+    "trtt_b200_conv3_wgrad": (_I, [_vp, _I, _vp, _I, _vp, _I, _vp, _vp, _vp, C.c_size_t, _I, _I,
+                                    _I, _I, _vp]),
+    "trtt_b200_unet_resample": (_I, [_vp, _vp, _I, _I, _I, _I, _I, _I, _I, _vp]),
+    "trtt_b200_unet_act_grad": (_I, [_vp, _vp, _L, _I, C.c_float, _vp]),
+    "trtt_b200_unet_pad_input": (_I, [_vp, _vp, _vp, C.c_float, _I, _I, _I, _I, _vp]),
+    "trtt_b200_unet_unpad": (_I, [_vp, _vp, C.c_float, _I, _I, _I, _I, _vp]),
+    "trtt_b200_unet_mse": (_I, [_vp, _vp, _vp, C.c_float, _vp, _I, _I, _I, _I, _vp]),
+    "trtt_b200_adam": (_I, [_vp, _vp, _vp, _vp, _L, C.c_float, C.c_float, C.c_float, C.c_float,
+                             _I, C.c_float, _vp]),
+    "trtt_b200_unet_status": (_I, [_vp]),
 }
 
 

@@ -1,0 +1,935 @@
+// unet.cu -- kernels of the learned warm start: a 3-level 3D U-Net whose
+// 3x3x3 convolutions (forward, input gradient, weight gradient) run on the
+// sm_100a tensor cores (tcgen05.mma, BF16 operands, FP32 accumulators in
+// tensor memory), plus its resampling, activation, loss and Adam kernels.
+//
+// Activation layout, "padded channels-last": a batch of nb volumes of
+// d x h x w voxels with C channels (C a multiple of 8) is stored as
+//   rows = nb (d+2)(h+2)(w+2) rows of C bf16,
+//   row ((v (d+2) + z)(h+2) + y)(w+2) + x, interior z in 1..d, y in 1..h,
+//   x in 1..w, and a one-voxel border that is zero and never written.
+// With that border the input row of tap (dz, dy, dx) of output row p is
+// p + dz (h+2)(w+2) + dy (w+2) + dx for EVERY p, so for a tile of
+// consecutive output rows the A operand of each tap is a contiguous run of
+// rows of one staged slab: the implicit GEMM needs no im2col copies, only a
+// different descriptor start address per tap.  Rows of a tile that fall on
+// the border are computed and discarded.
+//
+// Forward / input-gradient GEMM (k_conv3_fwd), per CTA 128*S output rows:
+//   D[row][n] += sum_{tap, k} X[row + off(tap)][k] W[n][tap][k]
+//   K loop in stages of (dz, 16 input channels): the stage holds a slab of
+//   128*S + 2(w+2) + 2 rows x 16 channels (chunk-major: each 8-channel chunk
+//   is a column of 16-byte rows, i.e. a stack of K-major core matrices) and
+//   the 9 (dy, dx) weight tiles of that dz; per stage 9*S MMAs of
+//   128 x N x 16.  The input gradient is the same kernel run on the output
+//   gradient with the weights transposed and flipped (tap -> 26 - tap).
+// Weight-gradient GEMM (k_conv3_wgrad), per CTA one (dz, dy) pair and a
+// range of rows:
+//   dW[co][tap][ci] = sum_row dY[row][co] X[row + off(tap)][ci]
+//   with both operands MN-major (the channels-last rows ARE the MN-major
+//   core matrices), M = 64 output channels (zero-padded), N = input
+//   channels, three accumulators (dx = -1, 0, 1); partial sums per row
+//   range are reduced by a second kernel.
+//
+// Every wait on an mbarrier is bounded in time; a kernel that gives up sets
+// a device error word (read by trtt_b200_unet_status), drains its copies,
+// frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "runtime.h"
+#include "tc100.cuh"
+#include "trtt_b200.h"
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr uint64_t kWaitNs = 2000000000ull;  // bound of every mbarrier wait (2 s)
+__device__ int g_unet_err;
+
+struct Grid3 {
+  int nb, d, h, w, hp, wp;
+  long plane, vol, rows;
+};
+
+Grid3 make_grid(int nb, int d, int h, int w)
+{
+  Grid3 g;
+  g.nb = nb; g.d = d; g.h = h; g.w = w;
+  g.hp = h + 2; g.wp = w + 2;
+  g.plane = (long)g.hp * g.wp;
+  g.vol = (long)(d + 2) * g.plane;
+  g.rows = (long)nb * g.vol;
+  return g;
+}
+
+__device__ __forceinline__ bool interior(const Grid3 &g, long p)
+{
+  if (p < 0 || p >= g.rows) return false;
+  const long r = p % g.vol;
+  const int z = (int)(r / g.plane);
+  const long q = r - (long)z * g.plane;
+  const int y = (int)(q / g.wp);
+  const int x = (int)(q - (long)y * g.wp);
+  return z >= 1 && z <= g.d && y >= 1 && y <= g.h && x >= 1 && x <= g.w;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+__device__ __forceinline__ float2 unpack_bf16x2(uint32_t u)
+{
+  __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162 *>(&u);
+  return __bfloat1622float2(v);
+}
+
+__device__ __forceinline__ float act(float v, float slope) { return v > 0.f ? v : v * slope; }
+
+// ---------------------------------------------------------------------------
+// forward / input-gradient convolution
+// ---------------------------------------------------------------------------
+enum { kFwdAct = 0, kFwdF32 = 1, kFwdHead = 2, kFwdGrad = 3 };
+
+struct FwdArgs {
+  const bf16 *x1, *x2;  // input channels [0, c1) from x1, [c1, c1 + c2) from x2
+  int c1, c2, groups;   // groups = (c1 + c2) / 16
+  const bf16 *wpack;    // [3 groups stages][9 taps][2 chunks][n][8]
+  const float *bias;    // [n] or null
+  int n, mode;
+  float slope;          // activation: v > 0 ? v : slope v (1 = identity)
+  void *y, *y2;
+  int n1, accumulate;   // kFwdGrad: channels [0, n1) -> y, [n1, n) -> y2
+  const float *resid;   // kFwdHead: y[p] = resid[p] + D[p][0] + bias[0]
+  Grid3 g;
+  long row0;            // first output row of tile 0
+  int rh, cs, stage_bytes, nstg;
+  uint32_t tmem_cols;
+};
+
+template <int S>
+__global__ void __launch_bounds__(128) k_conv3_fwd(const FwdArgs a)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar[4];
+  __shared__ uint32_t s_taddr;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long m0 = a.row0 + (long)blockIdx.x * (128 * S);
+  const int T = 3 * a.groups, n = a.n, nstg = a.nstg, pre = nstg - 2;
+  const uint32_t sbase = tc::smem_addr(smem);
+
+  if (tid == 0) {
+    for (int i = 0; i < nstg; ++i) tc::mbar_init(&mbar[i], 1);
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = s_taddr;
+
+  auto load = [&](int it, int buf) {
+    const int dz = it / a.groups - 1, ch = (it % a.groups) * 16;
+    const bf16 *src = a.x1;
+    int cst = a.c1, coff = ch;
+    if (ch >= a.c1) { src = a.x2; cst = a.c2; coff = ch - a.c1; }
+    const long hb = m0 + (long)dz * a.g.plane - a.g.wp - 1;
+    const uint32_t hs = sbase + (uint32_t)(buf * a.stage_bytes);
+    for (int e = tid; e < 2 * a.rh; e += 128) {
+      const int r = e >> 1, c = e & 1;
+      const long row = hb + r;
+      const bool ok = row >= 0 && row < a.g.rows;
+      const bf16 *p = ok ? src + row * cst + coff + c * 8 : src;
+      tc::cp16(hs + (uint32_t)(c * a.cs + r * 16), p, ok);
+    }
+    const uint32_t ws = hs + 2u * a.cs;
+    const bf16 *wsrc = a.wpack + (long)it * 9 * n * 16;
+    for (int e = tid; e < 9 * n * 2; e += 128) tc::cp16(ws + (uint32_t)e * 16u, wsrc + (long)e * 8, true);
+  };
+
+  const uint32_t idesc = tc::idesc_bf16(128, n, 0, 0);
+  bool bad = false;
+  for (int s = 0; s < pre; ++s) {
+    if (s < T) load(s, s);
+    tc::cp_commit();
+  }
+  for (int it = 0; it < T; ++it) {
+    const int nxt = it + pre;
+    if (nxt < T) {
+      if (it >= 2 && !tc::mbar_wait(&mbar[(it - 2) % nstg], ((it - 2) / nstg) & 1, kWaitNs)) bad = true;
+      if (!bad) load(nxt, nxt % nstg);
+    }
+    tc::cp_commit();
+    if (pre == 1) tc::cp_wait<1>(); else tc::cp_wait<2>();
+    tc::fence_async_smem();
+    if (__syncthreads_or(bad)) { bad = true; break; }
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const int buf = it % nstg;
+      const uint32_t hs = sbase + (uint32_t)(buf * a.stage_bytes), ws = hs + 2u * a.cs;
+      for (int t9 = 0; t9 < 9; ++t9) {
+        const int dy = t9 / 3, dx = t9 - 3 * (t9 / 3);
+        const uint64_t bd = tc::sdesc(ws + (uint32_t)(t9 * n * 32), (uint32_t)(n * 16), 128u);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const uint64_t ad = tc::sdesc(hs + (uint32_t)((dy * a.g.wp + dx + 128 * s) * 16), (uint32_t)a.cs, 128u);
+          tc::mma_bf16(tmem + (uint32_t)(s * n), ad, bd, idesc, (it > 0 || t9 > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&mbar[buf]);
+    }
+  }
+  if (!bad && T > 0) {
+    const int last = T - 1;
+    if (!tc::mbar_wait(&mbar[last % nstg], (last / nstg) & 1, kWaitNs)) bad = true;
+  }
+  bad = __syncthreads_or(bad);
+
+  if (!bad) {
+    tc::fence_after_sync();
+#pragma unroll 1
+    for (int s = 0; s < S; ++s) {
+      const long p = m0 + 128 * s + 32 * warp + lane;
+      const bool inside = interior(a.g, p);
+#pragma unroll 1
+      for (int j = 0; j < n; j += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(s * n + j), v);
+        if (!inside) continue;
+        if (a.bias && a.mode != kFwdGrad) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] += a.bias[j + i];
+        }
+        if (a.mode == kFwdAct) {
+          uint4 q0, q1;
+          q0.x = pack_bf16x2(act(v[0], a.slope), act(v[1], a.slope));
+          q0.y = pack_bf16x2(act(v[2], a.slope), act(v[3], a.slope));
+          q0.z = pack_bf16x2(act(v[4], a.slope), act(v[5], a.slope));
+          q0.w = pack_bf16x2(act(v[6], a.slope), act(v[7], a.slope));
+          q1.x = pack_bf16x2(act(v[8], a.slope), act(v[9], a.slope));
+          q1.y = pack_bf16x2(act(v[10], a.slope), act(v[11], a.slope));
+          q1.z = pack_bf16x2(act(v[12], a.slope), act(v[13], a.slope));
+          q1.w = pack_bf16x2(act(v[14], a.slope), act(v[15], a.slope));
+          uint4 *dst = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.y) + p * n + j);
+          dst[0] = q0;
+          dst[1] = q1;
+        } else if (a.mode == kFwdF32) {
+          float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(a.y) + p * n + j);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            dst[i] = make_float4(act(v[4 * i], a.slope), act(v[4 * i + 1], a.slope),
+                                 act(v[4 * i + 2], a.slope), act(v[4 * i + 3], a.slope));
+        } else if (a.mode == kFwdHead) {
+          if (j == 0) static_cast<float *>(a.y)[p] = a.resid[p] + v[0];
+        } else {  // kFwdGrad
+          bf16 *base;
+          int ld, c0;
+          if (j < a.n1) { base = static_cast<bf16 *>(a.y); ld = a.n1; c0 = j; }
+          else { base = static_cast<bf16 *>(a.y2); ld = n - a.n1; c0 = j - a.n1; }
+          uint4 *dst = reinterpret_cast<uint4 *>(base + p * ld + c0);
+          if (a.accumulate) {
+            const uint4 o0 = dst[0], o1 = dst[1];
+            const uint32_t ow[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const float2 f = unpack_bf16x2(ow[i]);
+              v[2 * i] += f.x;
+              v[2 * i + 1] += f.y;
+            }
+          }
+          uint4 q0, q1;
+          q0.x = pack_bf16x2(v[0], v[1]); q0.y = pack_bf16x2(v[2], v[3]);
+          q0.z = pack_bf16x2(v[4], v[5]); q0.w = pack_bf16x2(v[6], v[7]);
+          q1.x = pack_bf16x2(v[8], v[9]); q1.y = pack_bf16x2(v[10], v[11]);
+          q1.z = pack_bf16x2(v[12], v[13]); q1.w = pack_bf16x2(v[14], v[15]);
+          dst[0] = q0;
+          dst[1] = q1;
+        }
+      }
+    }
+  } else {
+    tc::cp_wait_all();
+    if (tid == 0) atomicExch(&g_unet_err, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, a.tmem_cols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient
+// ---------------------------------------------------------------------------
+constexpr int KT = 128;  // rows (K) per stage
+
+struct WgradArgs {
+  const bf16 *dy;       // [rows][cout]
+  const bf16 *x1, *x2;  // [rows][c1], [rows][c2]
+  int cout, c1, c2, cin;
+  float *part;          // [chunks][cout][27][cin]
+  Grid3 g;
+  long r0, r1;          // rows summed over
+  int steps;            // KT-row stages per CTA
+  int csa, csb, a_bytes, stage_bytes, nstg;
+  uint32_t tmem_cols;
+};
+
+__global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar[4];
+  __shared__ uint32_t s_taddr;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gidx = blockIdx.x, dzi = gidx / 3, dyi = gidx - 3 * (gidx / 3);
+  const long off = (long)(dzi - 1) * a.g.plane + (long)(dyi - 1) * a.g.wp;
+  const long qbeg = a.r0 + (long)blockIdx.y * a.steps * KT;
+  long rem = a.r1 - qbeg;
+  int T = rem <= 0 ? 0 : (int)((rem + KT - 1) / KT);
+  if (T > a.steps) T = a.steps;
+  const int nstg = a.nstg, pre = nstg - 2, cin = a.cin;
+  const int nca = a.cout / 8, ncb = cin / 8;
+  const uint32_t sbase = tc::smem_addr(smem);
+
+  if (tid == 0) {
+    for (int i = 0; i < nstg; ++i) tc::mbar_init(&mbar[i], 1);
+    tc::mbar_fence_init();
+  }
+  // zero the A chunks beyond cout once (the M = 64 MMAs read 8 chunks)
+  for (int b = 0; b < nstg; ++b) {
+    uint4 *z = reinterpret_cast<uint4 *>(smem + b * a.stage_bytes + nca * a.csa);
+    const int cnt = (8 - nca) * a.csa / 16;
+    for (int e = tid; e < cnt; e += 128) z[e] = make_uint4(0, 0, 0, 0);
+  }
+  if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = s_taddr;
+
+  auto load = [&](int it, int buf) {
+    const long q0 = qbeg + (long)it * KT;
+    const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
+    for (int e = tid; e < KT * nca; e += 128) {
+      const int r = e / nca, c = e - nca * (e / nca);
+      const long row = q0 + r;
+      const bool ok = row < a.r1;
+      const bf16 *p = ok ? a.dy + row * a.cout + c * 8 : a.dy;
+      tc::cp16(as + (uint32_t)(c * a.csa + r * 16), p, ok);
+    }
+    const long hb = q0 + off - 1;
+    for (int e = tid; e < (KT + 2) * ncb; e += 128) {
+      const int r = e / ncb, c = e - ncb * (e / ncb);
+      const long row = hb + r;
+      const bool ok = row >= 0 && row < a.g.rows;
+      const int ch = c * 8;
+      const bf16 *p = a.x1;
+      if (ok) p = (ch < a.c1) ? a.x1 + row * a.c1 + ch : a.x2 + row * a.c2 + (ch - a.c1);
+      tc::cp16(bs + (uint32_t)(c * a.csb + r * 16), p, ok);
+    }
+  };
+
+  const uint32_t idesc = tc::idesc_bf16(64, cin, 1, 1);
+  bool bad = false;
+  for (int s = 0; s < pre; ++s) {
+    if (s < T) load(s, s);
+    tc::cp_commit();
+  }
+  for (int it = 0; it < T; ++it) {
+    const int nxt = it + pre;
+    if (nxt < T) {
+      if (it >= 2 && !tc::mbar_wait(&mbar[(it - 2) % nstg], ((it - 2) / nstg) & 1, kWaitNs)) bad = true;
+      if (!bad) load(nxt, nxt % nstg);
+    }
+    tc::cp_commit();
+    if (pre == 1) tc::cp_wait<1>(); else tc::cp_wait<2>();
+    tc::fence_async_smem();
+    if (__syncthreads_or(bad)) { bad = true; break; }
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const int buf = it % nstg;
+      const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
+      for (int j = 0; j < 3; ++j) {
+#pragma unroll
+        for (int ks = 0; ks < KT / 16; ++ks) {
+          const uint64_t ad = tc::sdesc(as + (uint32_t)(ks * 256), 128u, (uint32_t)a.csa);
+          const uint64_t bd = tc::sdesc(bs + (uint32_t)((ks * 16 + j) * 16), 128u, (uint32_t)a.csb);
+          tc::mma_bf16(tmem + (uint32_t)(j * cin), ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&mbar[buf]);
+    }
+  }
+  if (!bad && T > 0) {
+    const int last = T - 1;
+    if (!tc::mbar_wait(&mbar[last % nstg], (last / nstg) & 1, kWaitNs)) bad = true;
+  }
+  bad = __syncthreads_or(bad);
+
+  if (!bad) {
+    tc::fence_after_sync();
+    // M = 64 accumulator: row co = 16 q + r sits in tensor-memory lane 32 q + r
+    const int co = 16 * warp + lane;
+    const bool mine = lane < 16 && co < a.cout;
+    float *dst = a.part + ((long)blockIdx.y * a.cout + (mine ? co : 0)) * 27 * cin;
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+      const int tap = gidx * 3 + j;
+#pragma unroll 1
+      for (int c0 = 0; c0 < cin; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * cin + c0), v);
+        if (mine) {
+          float4 *o = reinterpret_cast<float4 *>(dst + (long)tap * cin + c0);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (T > 0) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            else o[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      }
+    }
+  } else {
+    tc::cp_wait_all();
+    if (tid == 0) atomicExch(&g_unet_err, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, a.tmem_cols);
+  }
+}
+
+__global__ void k_sum_parts(const float *__restrict__ part, int chunks, long n, float *__restrict__ out)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int c = 0; c < chunks; ++c) s += part[(long)c * n + i];
+    out[i] = s;
+  }
+}
+
+// per-channel sum over all rows (bias gradient); rows of the border are zero
+__global__ void k_chan_sum(const bf16 *__restrict__ g, long rows, int c, float *__restrict__ out)
+{
+  extern __shared__ float acc[];
+  for (int i = threadIdx.x; i < c; i += blockDim.x) acc[i] = 0.f;
+  __syncthreads();
+  const int nch = c / 8;
+  float part[8];
+  int cur = -1;
+  for (int i = 0; i < 8; ++i) part[i] = 0.f;
+  // consecutive threads take consecutive 16-byte chunks; each thread keeps
+  // the chunk index fixed when the stride is a multiple of nch
+  const long total = rows * nch;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+    const int ch = (int)(e % nch);
+    if (ch != cur) {
+      if (cur >= 0)
+        for (int i = 0; i < 8; ++i) atomicAdd(&acc[cur * 8 + i], part[i]), part[i] = 0.f;
+      cur = ch;
+    }
+    const uint4 q = reinterpret_cast<const uint4 *>(g)[e];
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    for (int i = 0; i < 4; ++i) {
+      const float2 f = unpack_bf16x2(w[i]);
+      part[2 * i] += f.x;
+      part[2 * i + 1] += f.y;
+    }
+  }
+  if (cur >= 0)
+    for (int i = 0; i < 8; ++i) atomicAdd(&acc[cur * 8 + i], part[i]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < c; i += blockDim.x) atomicAdd(&out[i], acc[i]);
+}
+
+// ---------------------------------------------------------------------------
+// weight packing: FP32 master weights w[cout][27][cin] -> BF16 stage tiles
+// ---------------------------------------------------------------------------
+// forward:   pack[st = dz*G + gi][t9][c][n][k8] = w[n][dz*9 + t9][gi*16 + c*8 + k8],
+//            n < npack (rows >= cout zero), G = cin/16
+// transpose: the input-gradient weights, n = ci, k = co, tap flipped:
+//            pack[st = dz*G + gi][t9][c][n][k8] = w[gi*16 + c*8 + k8][26 - (dz*9 + t9)][n],
+//            G = cout_pad/16, n < cin
+__global__ void k_pack(const float *__restrict__ w, int cout, int cin, int npack, int kpack, int transpose,
+                       bf16 *__restrict__ out)
+{
+  const int G = kpack / 16;
+  const long total = (long)3 * G * 9 * 2 * npack * 8;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int k8 = (int)(e % 8);
+    const int nrow = (int)((e / 8) % npack);
+    const int c = (int)((e / (8L * npack)) % 2);
+    const int t9 = (int)((e / (16L * npack)) % 9);
+    const int st = (int)(e / (144L * npack));
+    const int dz = st / G, gi = st % G;
+    const int tap = dz * 9 + t9, k = gi * 16 + c * 8 + k8;
+    float v = 0.f;
+    if (!transpose) {
+      if (nrow < cout && k < cin) v = w[((long)nrow * 27 + tap) * cin + k];
+    } else {
+      if (k < cout && nrow < cin) v = w[((long)k * 27 + (26 - tap)) * cin + nrow];
+    }
+    out[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// resampling, activation gradient, input/output conversion, loss, Adam
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long prow(const Grid3 &g, int v, int z, int y, int x)
+{
+  return (((long)v * (g.d + 2) + z) * g.hp + y) * g.wp + x;
+}
+
+// thread per (coarse interior voxel, 8-channel chunk).  mode 0: coarse =
+// mean of the 8 children; 1: children (+)= coarse / 8 (its adjoint);
+// 2: children = coarse (nearest upsampling); 3: coarse (+)= sum of children.
+__global__ void k_resample(bf16 *fine, bf16 *coarse, int c, Grid3 gf, Grid3 gc, int mode, int accumulate)
+{
+  const int nch = c / 8;
+  const long total = (long)gc.nb * gc.d * gc.h * gc.w * nch;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int ch = (int)(e % nch);
+    long t = e / nch;
+    const int x = (int)(t % gc.w); t /= gc.w;
+    const int y = (int)(t % gc.h); t /= gc.h;
+    const int z = (int)(t % gc.d);
+    const int v = (int)(t / gc.d);
+    uint4 *cp = reinterpret_cast<uint4 *>(coarse + prow(gc, v, z + 1, y + 1, x + 1) * c) + ch;
+    float acc[8];
+    if (mode == 0 || mode == 3) {
+      for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+      for (int k = 0; k < 8; ++k) {
+        const long fr = prow(gf, v, 2 * z + 1 + (k >> 2), 2 * y + 1 + ((k >> 1) & 1), 2 * x + 1 + (k & 1));
+        const uint4 q = reinterpret_cast<const uint4 *>(fine + fr * c)[ch];
+        const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+        for (int i = 0; i < 4; ++i) {
+          const float2 f = unpack_bf16x2(w4[i]);
+          acc[2 * i] += f.x;
+          acc[2 * i + 1] += f.y;
+        }
+      }
+      const float sc = mode == 0 ? 0.125f : 1.f;
+      if (accumulate) {
+        const uint4 o = *cp;
+        const uint32_t w4[4] = {o.x, o.y, o.z, o.w};
+        for (int i = 0; i < 4; ++i) {
+          const float2 f = unpack_bf16x2(w4[i]);
+          acc[2 * i] = acc[2 * i] * sc + f.x;
+          acc[2 * i + 1] = acc[2 * i + 1] * sc + f.y;
+        }
+      } else {
+        for (int i = 0; i < 8; ++i) acc[i] *= sc;
+      }
+      *cp = make_uint4(pack_bf16x2(acc[0], acc[1]), pack_bf16x2(acc[2], acc[3]),
+                       pack_bf16x2(acc[4], acc[5]), pack_bf16x2(acc[6], acc[7]));
+    } else {
+      const uint4 q = *cp;
+      const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+      const float sc = mode == 1 ? 0.125f : 1.f;
+      for (int i = 0; i < 4; ++i) {
+        const float2 f = unpack_bf16x2(w4[i]);
+        acc[2 * i] = f.x * sc;
+        acc[2 * i + 1] = f.y * sc;
+      }
+      for (int k = 0; k < 8; ++k) {
+        const long fr = prow(gf, v, 2 * z + 1 + (k >> 2), 2 * y + 1 + ((k >> 1) & 1), 2 * x + 1 + (k & 1));
+        uint4 *fp = reinterpret_cast<uint4 *>(fine + fr * c) + ch;
+        float o[8];
+        for (int i = 0; i < 8; ++i) o[i] = acc[i];
+        if (accumulate) {
+          const uint4 p = *fp;
+          const uint32_t w5[4] = {p.x, p.y, p.z, p.w};
+          for (int i = 0; i < 4; ++i) {
+            const float2 f = unpack_bf16x2(w5[i]);
+            o[2 * i] += f.x;
+            o[2 * i + 1] += f.y;
+          }
+        }
+        *fp = make_uint4(pack_bf16x2(o[0], o[1]), pack_bf16x2(o[2], o[3]), pack_bf16x2(o[4], o[5]),
+                         pack_bf16x2(o[6], o[7]));
+      }
+    }
+  }
+}
+
+// g *= (y > 0 ? 1 : slope), 8 channels per thread
+__global__ void k_act_grad(bf16 *__restrict__ g, const bf16 *__restrict__ y, long n8, float slope)
+{
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n8; e += (long)gridDim.x * blockDim.x) {
+    const uint4 q = reinterpret_cast<const uint4 *>(g)[e];
+    const uint4 m = reinterpret_cast<const uint4 *>(y)[e];
+    const uint32_t gw[4] = {q.x, q.y, q.z, q.w}, mw[4] = {m.x, m.y, m.z, m.w};
+    uint32_t o[4];
+    for (int i = 0; i < 4; ++i) {
+      const float2 a = unpack_bf16x2(gw[i]), b = unpack_bf16x2(mw[i]);
+      o[i] = pack_bf16x2(b.x > 0.f ? a.x : a.x * slope, b.y > 0.f ? a.y : a.y * slope);
+    }
+    reinterpret_cast<uint4 *>(g)[e] = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+// dense x[nb][d][h][w] (FP32) -> xb padded [rows][16] BF16 (channel 0 =
+// scale x, channels 1..15 zero) and xf padded [rows] FP32 (scale x)
+__global__ void k_pad_input(const float *__restrict__ x, bf16 *__restrict__ xb, float *__restrict__ xf, Grid3 g,
+                            float scale)
+{
+  const long total = (long)g.nb * g.d * g.h * g.w;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    long t = e;
+    const int xx = (int)(t % g.w); t /= g.w;
+    const int yy = (int)(t % g.h); t /= g.h;
+    const int zz = (int)(t % g.d);
+    const int v = (int)(t / g.d);
+    const long p = prow(g, v, zz + 1, yy + 1, xx + 1);
+    const float val = scale * x[e];
+    uint4 *dst = reinterpret_cast<uint4 *>(xb + p * 16);
+    dst[0] = make_uint4(pack_bf16x2(val, 0.f), 0u, 0u, 0u);
+    dst[1] = make_uint4(0u, 0u, 0u, 0u);
+    if (xf) xf[p] = val;
+  }
+}
+
+// out (padded FP32) -> dense[nb][d][h][w] * scale
+__global__ void k_unpad(const float *__restrict__ xf, float *__restrict__ x, Grid3 g, float scale)
+{
+  const long total = (long)g.nb * g.d * g.h * g.w;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    long t = e;
+    const int xx = (int)(t % g.w); t /= g.w;
+    const int yy = (int)(t % g.h); t /= g.h;
+    const int zz = (int)(t % g.d);
+    const int v = (int)(t / g.d);
+    x[e] = scale * xf[prow(g, v, zz + 1, yy + 1, xx + 1)];
+  }
+}
+
+// mean squared error against dense target*scale: loss += sum r^2 / count,
+// dout[p][0] = 2 r / count (channels 1..15 untouched: zero)
+__global__ void k_mse(const float *__restrict__ out, const float *__restrict__ target, bf16 *__restrict__ dout,
+                      Grid3 g, float scale, double *__restrict__ loss)
+{
+  const long total = (long)g.nb * g.d * g.h * g.w;
+  const double inv = 1.0 / (double)total;
+  double acc = 0.0;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    long t = e;
+    const int xx = (int)(t % g.w); t /= g.w;
+    const int yy = (int)(t % g.h); t /= g.h;
+    const int zz = (int)(t % g.d);
+    const int v = (int)(t / g.d);
+    const long p = prow(g, v, zz + 1, yy + 1, xx + 1);
+    const float r = out[p] - scale * target[e];
+    acc += (double)r * r;
+    if (dout) dout[p * 16] = __float2bfloat16_rn((float)(2.0 * inv) * r);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) atomicAdd(loss, acc * inv);
+  }
+}
+
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, long n, float lr, float b1, float b2, float eps, float c1,
+                       float c2, float wd)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float gi = g[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int grid_for(long n, int threads = 256)
+{
+  long b = (n + threads - 1) / threads;
+  if (b > 148L * 16) b = 148L * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+uint32_t pow2_cols(int n)
+{
+  uint32_t c = 32;
+  while ((int)c < n) c <<= 1;
+  return c;
+}
+
+bool grid_ok(int nb, int d, int h, int w)
+{
+  return nb > 0 && d > 0 && h > 0 && w > 0 && (long)nb * (d + 2) * (long)(h + 2) * (w + 2) < (1L << 40);
+}
+
+constexpr int kSmemPerSM = 228 * 1024;
+
+// pad the dynamic shared memory so that at most 512 / tmem_cols CTAs can
+// be resident on one SM (their tensor-memory allocations then always fit)
+int residency_smem(int smem, uint32_t tmem_cols)
+{
+  const int max_ctas = 512 / (int)tmem_cols;
+  const int need = kSmemPerSM / (max_ctas + 1) + 1 - 1024;
+  return smem < need ? need : smem;
+}
+
+template <typename K>
+cudaError_t set_smem(K kern, int bytes)
+{
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+}  // namespace
+
+extern "C" {
+
+int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, const void *wpack, int n,
+                            const float *bias, int mode, float slope, void *y, void *y2, int n1,
+                            int accumulate, const float *resid, int nb, int d, int h, int w, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!x1 || !wpack || !y) return fail("conv3_forward: null pointer");
+  if (c1 <= 0 || c1 % 16 || c2 < 0 || c2 % 16 || (c2 > 0 && !x2))
+    return fail("conv3_forward: input channels must be multiples of 16");
+  if (n < 16 || n > 256 || n % 16) return fail("conv3_forward: output channels must be a multiple of 16 in [16, 256]");
+  if (mode < kFwdAct || mode > kFwdGrad) return fail("conv3_forward: bad mode");
+  if (mode == kFwdHead && !resid) return fail("conv3_forward: head mode needs the residual input");
+  if (mode == kFwdGrad && (n1 < 0 || n1 > n || n1 % 16 || (n1 < n && !y2)))
+    return fail("conv3_forward: bad channel split");
+  if (!grid_ok(nb, d, h, w)) return fail("conv3_forward: bad grid");
+  constexpr int S = 2;
+  FwdArgs a;
+  a.x1 = static_cast<const bf16 *>(x1);
+  a.x2 = static_cast<const bf16 *>(x2);
+  a.c1 = c1; a.c2 = c2; a.groups = (c1 + c2) / 16;
+  a.wpack = static_cast<const bf16 *>(wpack);
+  a.bias = bias; a.n = n; a.mode = mode; a.slope = slope;
+  a.y = y; a.y2 = y2; a.n1 = mode == kFwdGrad ? n1 : n; a.accumulate = accumulate;
+  a.resid = resid;
+  a.g = make_grid(nb, d, h, w);
+  a.row0 = a.g.plane;
+  a.rh = 128 * S + 2 * a.g.wp + 2;
+  a.cs = ((a.rh * 16 + 127) / 128) * 128 + 64;
+  a.stage_bytes = ((2 * a.cs + 288 * n + 1023) / 1024) * 1024;
+  a.nstg = 4 * a.stage_bytes <= 112 * 1024 ? 4 : 3;
+  int smem = a.nstg * a.stage_bytes;
+  a.tmem_cols = pow2_cols(S * n);
+  smem = residency_smem(smem, a.tmem_cols);
+  if (smem > 227 * 1024) return fail("conv3_forward: volume rows too long for the staged slab");
+  const long span = a.g.rows - 2 * a.g.plane;
+  const long tiles = (span + 128 * S - 1) / (128 * S);
+  if (tiles <= 0 || tiles > 0x7FFFFFFFL) return fail("conv3_forward: bad tile count");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  TRTT_CK(set_smem(k_conv3_fwd<S>, smem));
+  k_conv3_fwd<S><<<(unsigned)tiles, 128, smem, st>>>(a);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w)
+{
+  if (!grid_ok(nb, d, h, w) || cout <= 0 || cin <= 0) return 0;
+  const Grid3 g = make_grid(nb, d, h, w);
+  const long total = (g.rows - 2 * g.plane + KT - 1) / KT;
+  long chunks = 592 / 9;
+  if (chunks > total) chunks = total;
+  const long steps = (total + chunks - 1) / chunks;
+  chunks = (total + steps - 1) / steps;
+  return (size_t)chunks * cout * 27 * cin * sizeof(float);
+}
+
+int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2, float *dw,
+                          float *db, void *scratch, size_t scratch_bytes, int nb, int d, int h, int w,
+                          void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!dy || !x1 || !dw || !scratch) return fail("conv3_wgrad: null pointer");
+  const int cin = c1 + c2;
+  if (cout <= 0 || cout > 64 || cout % 16) return fail("conv3_wgrad: output channels must be 16, 32, 48 or 64");
+  if (c1 <= 0 || c1 % 16 || c2 < 0 || c2 % 16 || (c2 > 0 && !x2) || 3 * cin > 512)
+    return fail("conv3_wgrad: input channels must be multiples of 16 with 3 cin <= 512");
+  if (!grid_ok(nb, d, h, w)) return fail("conv3_wgrad: bad grid");
+  WgradArgs a;
+  a.dy = static_cast<const bf16 *>(dy);
+  a.x1 = static_cast<const bf16 *>(x1);
+  a.x2 = static_cast<const bf16 *>(x2);
+  a.cout = cout; a.c1 = c1; a.c2 = c2; a.cin = cin;
+  a.g = make_grid(nb, d, h, w);
+  a.r0 = a.g.plane;
+  a.r1 = a.g.rows - a.g.plane;
+  const long total = (a.r1 - a.r0 + KT - 1) / KT;
+  long chunks = 592 / 9;
+  if (chunks > total) chunks = total;
+  const long steps = (total + chunks - 1) / chunks;
+  chunks = (total + steps - 1) / steps;
+  if (steps > 0x7FFFFFFFL) return fail("conv3_wgrad: too many rows");
+  a.steps = (int)steps;
+  const size_t need = (size_t)chunks * cout * 27 * cin * sizeof(float);
+  if (scratch_bytes < need) return fail("conv3_wgrad: scratch too small");
+  a.part = static_cast<float *>(scratch);
+  const int nca = cout / 8, ncb = cin / 8;
+  const int pad_a = nca == 2 ? 64 : nca == 4 ? 32 : 16;
+  const int pad_b = ncb == 2 ? 64 : ncb == 4 ? 32 : 16;
+  a.csa = KT * 16 + pad_a;
+  a.csb = (((KT + 2) * 16 + 127) / 128) * 128 + pad_b;
+  a.a_bytes = ((8 * a.csa + 127) / 128) * 128;
+  a.stage_bytes = ((a.a_bytes + ncb * a.csb + 1023) / 1024) * 1024;
+  a.nstg = 4 * a.stage_bytes <= 112 * 1024 ? 4 : 3;
+  a.tmem_cols = pow2_cols(3 * cin);
+  int smem = residency_smem(a.nstg * a.stage_bytes, a.tmem_cols);
+  if (smem > 227 * 1024) return fail("conv3_wgrad: stage too large");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  TRTT_CK(set_smem(k_conv3_wgrad, smem));
+  dim3 grid(9, (unsigned)chunks);
+  k_conv3_wgrad<<<grid, 128, smem, st>>>(a);
+  const long nw = (long)cout * 27 * cin;
+  k_sum_parts<<<grid_for(nw), 256, 0, st>>>(a.part, (int)chunks, nw, dw);
+  count_launch(2);
+  if (db) {
+    TRTT_CK(cudaMemsetAsync(db, 0, sizeof(float) * cout, st));
+    k_chan_sum<<<148 * 4, 256, sizeof(float) * cout, st>>>(a.dy, a.g.rows, cout, db);
+    count_launch();
+  }
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_conv3_pack(const float *w, int cout, int cin, int transpose, void *wpack, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!w || !wpack) return fail("conv3_pack: null pointer");
+  if (cout <= 0 || cin <= 0 || cin % 16) return fail("conv3_pack: cin must be a multiple of 16");
+  const int coutp = (cout + 15) / 16 * 16;
+  const int npack = transpose ? cin : coutp;
+  const int kpack = transpose ? coutp : cin;
+  const long total = (long)27 * npack * kpack;
+  k_pack<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, cout, cin, npack, kpack, transpose,
+                                                                         static_cast<bf16 *>(wpack));
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_resample(void *fine, void *coarse, int c, int nb, int d, int h, int w, int mode,
+                            int accumulate, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!fine || !coarse) return fail("unet_resample: null pointer");
+  if (c <= 0 || c % 8 || d % 2 || h % 2 || w % 2 || mode < 0 || mode > 3)
+    return fail("unet_resample: channels must be a multiple of 8 and the fine grid even");
+  if (!grid_ok(nb, d, h, w)) return fail("unet_resample: bad grid");
+  const Grid3 gf = make_grid(nb, d, h, w), gc = make_grid(nb, d / 2, h / 2, w / 2);
+  const long total = (long)nb * (d / 2) * (h / 2) * (w / 2) * (c / 8);
+  k_resample<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<bf16 *>(fine), static_cast<bf16 *>(coarse), c, gf, gc, mode, accumulate);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_act_grad(void *g, const void *y, long rows, int c, float slope, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!g || !y || rows <= 0 || c <= 0 || c % 8) return fail("unet_act_grad: bad arguments");
+  const long n8 = rows * (c / 8);
+  k_act_grad<<<grid_for(n8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<bf16 *>(g), static_cast<const bf16 *>(y), n8, slope);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_pad_input(const float *x, void *xb, float *xf, float scale, int nb, int d, int h, int w,
+                             void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!x || !xb || !grid_ok(nb, d, h, w)) return fail("unet_pad_input: bad arguments");
+  const Grid3 g = make_grid(nb, d, h, w);
+  k_pad_input<<<grid_for((long)nb * d * h * w), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      x, static_cast<bf16 *>(xb), xf, g, scale);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_unpad(const float *xf, float *x, float scale, int nb, int d, int h, int w, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!x || !xf || !grid_ok(nb, d, h, w)) return fail("unet_unpad: bad arguments");
+  const Grid3 g = make_grid(nb, d, h, w);
+  k_unpad<<<grid_for((long)nb * d * h * w), 256, 0, static_cast<cudaStream_t>(stream)>>>(xf, x, g, scale);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_mse(const float *out, const float *target, void *dout, float scale, double *loss, int nb,
+                       int d, int h, int w, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!out || !target || !loss || !grid_ok(nb, d, h, w)) return fail("unet_mse: bad arguments");
+  const Grid3 g = make_grid(nb, d, h, w);
+  k_mse<<<grid_for((long)nb * d * h * w), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      out, target, static_cast<bf16 *>(dout), g, scale, loss);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_adam(float *w, const float *g, float *m, float *v, long n, float lr, float b1, float b2, float eps,
+                   int step, float weight_decay, void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!w || !g || !m || !v || n <= 0 || step < 1) return fail("adam: bad arguments");
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, g, m, v, n, lr, b1, b2, eps, c1, c2,
+                                                                     weight_decay);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_status(void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  int e = 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  TRTT_CK(cudaMemcpyFromSymbolAsync(&e, g_unet_err, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
+  TRTT_CK(cudaStreamSynchronize(st));
+  if (e) {
+    const int zero = 0;
+    TRTT_CK(cudaMemcpyToSymbolAsync(g_unet_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st));
+    TRTT_CK(cudaStreamSynchronize(st));
+    return fail("tensor-core convolution gave up waiting for its MMAs (time limit reached)");
+  }
+  return 0;
+}
+
+}  // extern "C"
