@@ -268,9 +268,9 @@ def run_b200(args):
     nvox, npix = N ** 3, ND * ND
     fwd_avg, back_avg = statistics.mean(fwd_ms), statistics.mean(back_ms)
     if back_avg >= fwd_avg:
-        kern, kms = "k_back3d_col (transpose, column gather)", back_avg
+        kern, kms = "k_back3d_col_fast (transpose, column gather)", back_avg
     else:
-        kern, kms = "k_fwd3d_band (direct, detector-row bands)", fwd_avg
+        kern, kms = "k_fwd3d_band_fast (direct, detector-row bands)", fwd_avg
     alg_bytes = VIEWS * (4 * nvox + 4 * npix)
     peaks = {}
     try:
