@@ -384,9 +384,12 @@ def main(argv=None):
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--workload", default="pair3d",
-                    choices=["pair3d", "parallel2d_recon", "fan2d", "cone3d_recon", "gates4d"],
+                    choices=["pair3d", "parallel2d_recon", "fan2d", "cone3d_recon", "gates4d",
+                             "learned_warmstart", "learned_eval"],
                     help="pair3d (default) is the benchmark line; the others measure the "
                          "remaining configurations (yoricktrtt_b200/workloads.py)")
+    ap.add_argument("--param", action="append", default=[], metavar="KEY=VALUE",
+                    help="keyword argument of a --workload function (repeatable)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
@@ -396,7 +399,14 @@ def main(argv=None):
         import torch
         from yoricktrtt_b200 import workloads
         torch.cuda.set_device(_env_int("LOCAL_RANK", 0))
-        res = getattr(workloads, args.workload)()
+        kw = {}
+        for kv in args.param:
+            k, v = kv.split("=", 1)
+            try:
+                kw[k] = json.loads(v)
+            except ValueError:
+                kw[k] = v
+        res = getattr(workloads, args.workload)(**kw)
         print(json.dumps({"workload": args.workload, **res}))
         return 0
     return run_b200(args)

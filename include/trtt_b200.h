@@ -199,6 +199,9 @@ int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps)
 /* 1 if every view of the plan uses the column-factorised kernels. */
 int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
 
+/* shape[0..6] = nx, ny, nz, nu, nv, nviews, number of gates. */
+int trtt_b200_plan3d_shape(const trtt_b200_plan3d *plan, long *shape);
+
 int trtt_b200_plan3d_destroy(trtt_b200_plan3d *plan);
 
 typedef struct trtt_b200_plan2d trtt_b200_plan2d;
@@ -268,6 +271,29 @@ int trtt_b200_tv(const float *z, long nx, long ny, long nz, double eps, double m
 int trtt_b200_spline_sample(const float *x, float *z, float *tmp, long nx, long ny, long nz,
                             void *stream);
 
+/* Native regularised reconstruction on a 3D plan (one volume, no gates):
+ * minimise 1/2 (Hx - y)' W (Hx - y) + mu TV(S x) (w may be NULL: W = I;
+ * TV and S as in trtt_b200_tv / trtt_b200_spline_sample) under
+ * lower <= x <= upper (+-HUGE_VAL: no bound) by VMLM-B with `mem` pairs,
+ * projected Armijo backtracking (at most 30 trials) and the stopping rule
+ * |f_k - f_k+1| <= frtol max(|f_k|, |f_k+1|), at most maxiter iterations.
+ * The cost is that of Tomography_3D/Ytrtt3D_optim.i:128-234, minimised
+ * there by OptimPack's op_mnb (Tomography_3D/Ytrtt3D_optim.i:663).
+ * x (device, `layout`) holds the start and receives the result; y, w are
+ * device detector stacks [view][nv][nu].  f_hist / t_hist (host, may be
+ * NULL) receive maxiter + 1 objective values / wall-clock seconds since the
+ * start (entry k after iteration k).  info->converged: 1 stopping rule met,
+ * 2 zero projected gradient, 0 iteration limit, -1 line search failed.
+ * Work buffers are allocated for the call (about 2 mem + 14 volumes). */
+typedef struct {
+  int iterations, evaluations, converged;
+  double f_first, f_last, seconds;
+} trtt_b200_vmlmb_info;
+int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, float *x, int layout,
+                      double mu, double eps, double lower, double upper, int mem, int maxiter,
+                      double frtol, double *f_hist, double *t_hist, trtt_b200_vmlmb_info *info,
+                      void *stream);
+
 /* Allocation-free cone-beam direct projector.  No counterpart in the
  * reference (whose plugin allocates on the host per voxel).  For callers that
  * cannot call cudaMalloc: code running while a stream is captured into a
@@ -330,6 +356,8 @@ int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, float *sino,
  * unet_unpad: padded FP32 [rows] -> dense FP32 times scale.
  * unet_mse: *loss += mean over voxels of (out - scale target)^2 (FP64) and,
  *   if dout is not NULL, dout[row][0] = its derivative (BF16 [rows][16]).
+ * unet_add_output_grad: dout[row][0] += coef g for a dense FP32 g[nb][d][h][w]
+ *   (an extra loss term on the network output).
  * adam: Adam step number `step` (>= 1) with decoupled-free L2 term
  *   weight_decay * w added to the gradient.
  * unet_status: -1 if a convolution kernel gave up waiting for its tensor-core
@@ -352,6 +380,8 @@ int trtt_b200_unet_unpad(const float *xf, float *x, float scale, int nb, int d, 
                          void *stream);
 int trtt_b200_unet_mse(const float *out, const float *target, void *dout, float scale, double *loss,
                        int nb, int d, int h, int w, void *stream);
+int trtt_b200_unet_add_output_grad(void *dout, const float *g, float coef, int nb, int d, int h, int w,
+                                   void *stream);
 int trtt_b200_adam(float *w, const float *g, float *m, float *v, long n, float lr, float b1, float b2,
                    float eps, int step, float weight_decay, void *stream);
 int trtt_b200_unet_status(void *stream);

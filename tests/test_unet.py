@@ -203,13 +203,16 @@ def test_unet_forward_and_gradients_match_cpu(lib):
 
 @pytest.mark.gpu
 def test_unet_training_reduces_loss(lib):
-    """A few Adam steps on one fixed pair lower the loss (smoke test of the
-    training loop on the tensor-core kernels)."""
+    """Adam steps on one fixed pair lower the loss (smoke test of the
+    training loop on the tensor-core kernels): the target is the input
+    plus a smooth offset field."""
     from yoricktrtt_b200.unet import UNet3D
     g = torch.Generator().manual_seed(11)
-    x = torch.rand(1, 16, 16, 16, generator=g).cuda()
-    t = (0.5 * x + 0.2).contiguous()
-    net = UNet3D(scale=1.0, seed=1, lr=1e-2)
-    losses = [float(net.train_step(x, t)) for _ in range(40)]
+    x = torch.rand(1, 16, 16, 16, generator=g)
+    zz = torch.linspace(0, 1, 16)
+    t = (x + 0.2 + 0.1 * zz[None, :, None, None]).contiguous()
+    net = UNet3D(scale=1.0, seed=1, lr=2e-3)
+    losses = [float(net.train_step(x.cuda(), t.cuda())) for _ in range(150)]
     net.status()
-    assert losses[-1] < 0.6 * losses[0]
+    assert all(np.isfinite(losses))
+    assert losses[-1] < 0.3 * losses[0]

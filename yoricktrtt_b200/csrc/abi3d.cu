@@ -179,6 +179,20 @@ extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
   return pl && pl->factorized ? 1 : 0;
 }
 
+extern "C" int trtt_b200_plan3d_shape(const trtt_b200_plan3d *pl, long *shape)
+{
+  clear_error();
+  if (!pl || !shape) return fail("plan3d_shape: null argument");
+  shape[0] = pl->P.nx;
+  shape[1] = pl->P.ny;
+  shape[2] = pl->P.nz;
+  shape[3] = pl->P.nu;
+  shape[4] = pl->P.nv;
+  shape[5] = pl->nviews;
+  shape[6] = pl->nt;
+  return 0;
+}
+
 static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long view0,
                     long nview, int layout, void *stream, bool forward)
 {

@@ -642,6 +642,21 @@ __global__ void k_mse(const float *__restrict__ out, const float *__restrict__ t
   }
 }
 
+// dout[p][0] += coef g (dense FP32 g[nb][d][h][w])
+__global__ void k_add_out_grad(bf16 *__restrict__ dout, const float *__restrict__ g, Grid3 gr, float coef)
+{
+  const long total = (long)gr.nb * gr.d * gr.h * gr.w;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    long t = e;
+    const int xx = (int)(t % gr.w); t /= gr.w;
+    const int yy = (int)(t % gr.h); t /= gr.h;
+    const int zz = (int)(t % gr.d);
+    const int v = (int)(t / gr.d);
+    bf16 *o = dout + prow(gr, v, zz + 1, yy + 1, xx + 1) * 16;
+    *o = __float2bfloat16_rn(__bfloat162float(*o) + coef * g[e]);
+  }
+}
+
 __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, long n, float lr, float b1, float b2, float eps, float c1,
                        float c2, float wd)
@@ -896,6 +911,20 @@ int trtt_b200_unet_mse(const float *out, const float *target, void *dout, float 
   const Grid3 g = make_grid(nb, d, h, w);
   k_mse<<<grid_for((long)nb * d * h * w), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       out, target, static_cast<bf16 *>(dout), g, scale, loss);
+  count_launch();
+  TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_unet_add_output_grad(void *dout, const float *g, float coef, int nb, int d, int h, int w,
+                                   void *stream)
+{
+  using namespace trtt;
+  clear_error();
+  if (!dout || !g || !grid_ok(nb, d, h, w)) return fail("unet_add_output_grad: bad arguments");
+  const Grid3 gr = make_grid(nb, d, h, w);
+  k_add_out_grad<<<grid_for((long)nb * d * h * w), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<bf16 *>(dout), g, gr, coef);
   count_launch();
   TRTT_CK(cudaGetLastError());
   return 0;

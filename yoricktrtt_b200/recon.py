@@ -205,78 +205,153 @@ class VMLMBInfo:
     reason: str = ""
 
 
+_REASONS = {1: "relative objective change below frtol", 2: "projected gradient is zero",
+            0: "", -1: "line search failed"}
+
+
+def vmlmb_native(proj, y, w=None, x0=None, mu=0.0, eps=1e-3, lower=0.0, upper=None, mem=5,
+                 maxiter=100, frtol=1e-6, layout="xyz", stream=None):
+    """VMLM-B + TV on a Projector3D with the native solver
+    (trtt_b200_recon3d): the cost of ``Objective`` (spline=True) and the
+    rules of ``vmlmb``, driven from C++ with fused vector kernels.
+    Returns (x, VMLMBInfo) like ``vmlmb``."""
+    torch = _torch()
+    from .projectors import LAYOUTS
+    if proj.nt != 1:
+        raise ValueError("vmlmb_native: gated (4D) projectors are not supported")
+    shape = proj.volume_shape(layout)
+    x = (torch.zeros(shape, device=y.device) if x0 is None else x0).clone().contiguous()
+    if tuple(x.shape) != tuple(shape) or x.dtype != torch.float32:
+        raise ValueError(f"x0 must be float32 with shape {tuple(shape)}")
+    y = y.contiguous()
+    w = None if w is None else w.contiguous()
+    fh = np.zeros(maxiter + 1)
+    th = np.zeros(maxiter + 1)
+    info_c = _lib.VMLMBInfoC()
+    st = C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
+    rc = _lib.load().trtt_b200_recon3d(
+        proj._h, _ptr(y), _ptr(w) if w is not None else None, _ptr(x), LAYOUTS[layout], float(mu),
+        float(eps), -math.inf if lower is None else float(lower), math.inf if upper is None else float(upper),
+        int(mem), int(maxiter), float(frtol), fh.ctypes.data_as(C.POINTER(C.c_double)),
+        th.ctypes.data_as(C.POINTER(C.c_double)), C.byref(info_c), st)
+    _lib.check(rc, "trtt_b200_recon3d")
+    k = info_c.iterations
+    info = VMLMBInfo(iterations=k, evaluations=info_c.evaluations, f=fh[:k + 1].tolist(),
+                     times=th[:k + 1].tolist(), converged=info_c.converged > 0,
+                     reason=_REASONS.get(info_c.converged, ""))
+    return x, info
+
+
+def dot_dev(a, b):
+    """FP64-accumulated inner product left on the device (0-dim float64
+    tensor), so that several can be read back with one synchronisation."""
+    torch = _torch()
+    out = torch.zeros((), dtype=torch.float64, device=a.device)
+    _lib.check(_lib.load().trtt_b200_dot(_ptr(a), _ptr(b), a.numel(), _ptr(out), _stream()),
+               "trtt_b200_dot")
+    return out
+
+
+def _fetch(*vals):
+    """Read several device scalars with one synchronisation."""
+    torch = _torch()
+    return torch.stack([v.reshape(()) for v in vals]).tolist()
+
+
 def vmlmb(fg, x0, lower=0.0, upper=None, mem=5, maxiter=100, frtol=1e-6, armijo=1e-4,
           max_backtrack=30, callback=None):
     """VMLM-B: L-BFGS restricted to the free variables of the box
     lower <= x <= upper, projected Armijo backtracking with safeguarded
     quadratic steps, stop when |f_k - f_{k+1}| <= frtol max(|f_k|,|f_{k+1}|).
 
-    The same rules are restated in FP64 on the CPU by oracle/recon_oracle.py.
-    Returns (x, VMLMBInfo)."""
+    Inner products are FP64 (trtt_b200_dot) and stay on the device: the
+    two-loop recursion applies its coefficients as device scalars, and the
+    host reads back only the values it branches on (a few synchronisations
+    per iteration).  The same rules are restated in FP64 on the CPU by
+    oracle/recon_oracle.py.  Returns (x, VMLMBInfo)."""
     torch = _torch()
     lo = -math.inf if lower is None else float(lower)
     hi = math.inf if upper is None else float(upper)
-    acc = _Scalar(x0.device)
 
     def clip(v):
         return v.clamp(min=None if lo == -math.inf else lo, max=None if hi == math.inf else hi)
-
-    def d64(a, b):
-        return dot(a, b, acc)
 
     t0 = time.perf_counter()
     x = clip(x0.clone())
     f, g = fg(x)
     info = VMLMBInfo(evaluations=1, f=[f], times=[0.0])
     S, Y = [], []
+    cand = None  # (s, y) of the last step, kept if s'y > 0
     for it in range(1, maxiter + 1):
-        free = torch.ones_like(x)
+        blocked = None
         if lo > -math.inf:
-            free[(x <= lo) & (g > 0)] = 0.0
+            blocked = (x <= lo) & (g > 0)
         if hi < math.inf:
-            free[(x >= hi) & (g < 0)] = 0.0
+            b2 = (x >= hi) & (g < 0)
+            blocked = b2 if blocked is None else blocked | b2
+        free = torch.ones_like(x) if blocked is None else (~blocked).to(x.dtype)
         pg = g * free
-        pgn = math.sqrt(d64(pg, pg))
+        # one read-back: |pg|^2, |x|^2, s'y of the candidate pair and the
+        # free-restricted s'y of every stored pair and of the candidate
+        pend = list(zip(S, Y)) + ([cand] if cand is not None else [])
+        sfs = [(s * free, y * free) for s, y in pend]
+        vals = [dot_dev(pg, pg), dot_dev(x, x)]
+        if cand is not None:
+            vals.append(dot_dev(cand[0], cand[1]))
+        vals += [dot_dev(sf, yf) for sf, yf in sfs]
+        got = _fetch(*vals)
+        pgn, xn = math.sqrt(got[0]), math.sqrt(got[1])
+        sys_free = got[3:] if cand is not None else got[2:]
+        if cand is not None:
+            if got[2] > 0.0:
+                S.append(cand[0])
+                Y.append(cand[1])
+            else:
+                sfs.pop()
+                sys_free.pop()
+            cand = None
+            if len(S) > mem:
+                S.pop(0)
+                Y.pop(0)
+                sfs.pop(0)
+                sys_free.pop(0)
         if pgn == 0.0:
             info.converged, info.reason = True, "projected gradient is zero"
             break
         # two-loop recursion on the free subspace
         q = pg.clone()
         used = []
-        for s, y in reversed(list(zip(S, Y))):
-            sf, yf = s * free, y * free
-            sy = d64(sf, yf)
+        for (sf, yf), sy in reversed(list(zip(sfs, sys_free))):
             if sy <= 0.0:
                 continue
-            a = d64(sf, q) / sy
+            a = dot_dev(sf, q) / sy
             q -= a * yf
             used.append((sf, yf, sy, a))
         if used:
             sf, yf, sy, _ = used[0]
-            q *= sy / d64(yf, yf)
+            q *= sy / dot_dev(yf, yf)
             for sf, yf, sy, a in reversed(used):
-                b = d64(yf, q) / sy
+                b = dot_dev(yf, q) / sy
                 q += (a - b) * sf
             d = -(q * free)
             alpha = 1.0
         else:
             d = -pg
-            xn = math.sqrt(d64(x, x))
             alpha = (0.1 * xn if xn > 0 else 1.0) / pgn
-        gd = d64(g, d)
+        gd = _fetch(dot_dev(g, d))[0]
         if gd >= 0.0:  # not a descent direction: restart with the gradient
             S.clear()
             Y.clear()
             d = -pg
-            xn = math.sqrt(d64(x, x))
             alpha = (0.1 * xn if xn > 0 else 1.0) / pgn
-            gd = d64(g, d)
+            gd = _fetch(dot_dev(g, d))[0]
         for _ in range(max_backtrack):
             xt = clip(x + alpha * d)
+            step = xt - x
+            gs = dot_dev(g, step)
             ft, gt = fg(xt)
             info.evaluations += 1
-            step = xt - x
-            if ft <= f + armijo * d64(g, step):
+            if ft <= f + armijo * _fetch(gs)[0]:
                 break
             # safeguarded quadratic interpolation of phi(alpha)
             denom = 2.0 * (ft - f - gd * alpha)
@@ -285,14 +360,7 @@ def vmlmb(fg, x0, lower=0.0, upper=None, mem=5, maxiter=100, frtol=1e-6, armijo=
         else:
             info.reason = "line search failed"
             break
-        s = xt - x
-        yv = gt - g
-        if d64(s, yv) > 0.0:
-            S.append(s)
-            Y.append(yv)
-            if len(S) > mem:
-                S.pop(0)
-                Y.pop(0)
+        cand = (step, gt - g)
         fprev = f
         x, f, g = xt, ft, gt
         info.iterations = it

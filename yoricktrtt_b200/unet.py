@@ -255,9 +255,12 @@ class UNet3D:
 
     __call__ = forward
 
-    def backward(self, x, target):
+    def backward(self, x, target, extra_grad=None):
         """Forward pass, loss mean((out - scale target)^2) and the gradients of
-        every parameter (left in self._grads).  Returns the loss (device)."""
+        every parameter (left in self._grads).  ``extra_grad`` (dense FP32
+        like x): the gradient of an additional loss term with respect to the
+        network output (in the units of x), added to the MSE gradient.
+        Returns the MSE loss (device)."""
         lib = _lib.load()
         x = x.contiguous()
         target = target.contiguous()
@@ -267,6 +270,10 @@ class UNet3D:
         self._loss.zero_()
         _lib.check(lib.trtt_b200_unet_mse(_p(out), _p(target), _p(G["dout"]), self.scale, _p(self._loss),
                                           nb, d, h, w, _stream()), "unet_mse")
+        if extra_grad is not None:
+            eg = extra_grad.contiguous()
+            _lib.check(lib.trtt_b200_unet_add_output_grad(_p(G["dout"]), _p(eg), 1.0 / self.scale, nb, d, h, w,
+                                                          _stream()), "unet_add_output_grad")
         self._conv_dw("head", G["dout"], A["d1b"], None)
         self._conv_dx("head", G["dout"], G["d1b"], None)
         self._act_grad(G["d1b"], A["d1b"])
@@ -316,8 +323,8 @@ class UNet3D:
                                               1e-8, self.step_count, self.weight_decay, _stream()), "adam")
         self._pack_all()
 
-    def train_step(self, x, target):
-        loss = self.backward(x, target)
+    def train_step(self, x, target, extra_grad=None):
+        loss = self.backward(x, target, extra_grad)
         self.step()
         return loss
 
