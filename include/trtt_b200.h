@@ -196,6 +196,12 @@ int trtt_b200_plan3d_status(trtt_b200_plan3d *plan, void *stream);
 #define TRTT_B200_TILES_PULL (-2)
 int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps);
 
+/* Band kernel variant (closed-form model): cols = 1 one column at a time
+ * (default), cols = 2 neighbouring columns in pairs, spread into the band
+ * with one atomic per cell of the union of their footprints.  -1 if the
+ * pair kernel's shared memory (band + 2 profiles per warp) does not fit. */
+int trtt_b200_plan3d_set_columns(trtt_b200_plan3d *plan, int cols);
+
 /* 1 if every view of the plan uses the column-factorised kernels. */
 int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
 

@@ -176,10 +176,17 @@ def test_view_subrange_and_tiles(oracle_port):
     pr = Projector3D(sc)
     xt = torch.tensor(vol, dtype=torch.float32, device="cuda")
     full = pr.forward(xt).cpu().numpy()
-    for rows, warps in [(4, 2), (7, 4), (36, 16), (-1, 0), (-2, 0), (0, 0)]:
-        pr.set_tiles(rows, warps)
+    for tiles in [(4, 2), (7, 4), (36, 16), (-1, 0), (-2, 0), (0, 0), (4, 2, 2), (7, 4, 2), (36, 16, 2),
+                  (0, 0, 2)]:
+        pr.set_tiles(*tiles)
         part = pr.forward(xt, view0=2, nview=3).cpu().numpy()
-        assert rel_l2(part, full[2:5]) <= 1e-6, (rows, warps)
+        assert rel_l2(part, full[2:5]) <= 1e-6, tiles
+    pr.set_tiles(0, 0, 2)
+    ref_f = np.zeros((sc.nviews, sc.nv, sc.nu))
+    for v in range(sc.nviews):
+        oracle_port.cb3d(ref_f[v], vol, sc, v, 0)
+    assert rel_l2(pr.forward(xt).double().cpu().numpy(), ref_f) <= TOL
+    pr.set_tiles(0, 0)
     y = torch.rand(sc.nviews, sc.nv, sc.nu, device="cuda")
     a = pr.backward(y[2:5], view0=2, nview=3).double().cpu().numpy()
     ref = np.zeros_like(vol)

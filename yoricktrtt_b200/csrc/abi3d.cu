@@ -27,6 +27,7 @@ struct trtt_b200_plan3d {
   int nt = 1;
   int band_rows = 0, warps = 16;
   int pull = 0;  // 1: atomic-free band kernel (closed-form model, nu <= 512)
+  int cols = 1;  // 2: column-pair band kernel (closed-form model)
   bool factorized = true;
   DevBuf views, cum, gate_ptr, entries, scratch, err;
   std::vector<View3D> hviews;
@@ -174,6 +175,19 @@ extern "C" int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *pl, int band_rows, i
   return 0;
 }
 
+extern "C" int trtt_b200_plan3d_set_columns(trtt_b200_plan3d *pl, int cols)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_columns: null plan");
+  if (cols != 1 && cols != 2) return fail("plan3d_set_columns: cols must be 1 or 2");
+  if (cols == 2 && pl->band_rows > 0) {
+    const long smem = 4L * ((long)pl->band_rows * pl->P.nu + 2L * pl->warps * pl->P.nu + 2L * pl->warps * pl->band_rows);
+    if (smem > 227L * 1024) return fail("plan3d_set_columns: band does not fit in shared memory");
+  }
+  pl->cols = cols;
+  return 0;
+}
+
 extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
 {
   return pl && pl->factorized ? 1 : 0;
@@ -231,6 +245,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
     L.band_rows = pl->factorized ? pl->band_rows : 0;
     L.warps = pl->warps;
     L.pull = pl->pull;
+    L.cols = pl->cols;
     L.err = pl->err.as<int>();
     TRTT_CK(launch_fwd3d(L, st));
     count_launch();

@@ -31,6 +31,7 @@ struct Fwd3DLaunch {
   int band_rows;         // > 0: band kernel (factorised views); 0: per-voxel
   int warps;             // warps per CTA of the band kernel
   int pull = 0;          // closed-form model, nu <= 512: atomic-free band kernel
+  int cols = 1;          // closed-form model: 2 = column-pair band kernel
   int *err;              // device error flags
 };
 

@@ -153,6 +153,154 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   }
 }
 
+// Profile of one column: prof[u] += sum_k rho_k x_k (F(e_{u+1,k}) - F(e_{u,k}))
+// (shared-memory atomics), returns the warp-uniform cell range [lo, hi).
+template <int GEOM>
+__device__ __forceinline__ void column_profile(const Params3D &P, const View3D &V, const float *__restrict__ vol,
+                                               long gate_stride, const ColGeo<MODEL_CUBIC> &cc, int col,
+                                               float *prof, int lane, int &lo_out, int &hi_out)
+{
+  const int nz = P.nz;
+  int lo = INT_MAX, hi = INT_MIN;
+  const long cbase = (long)col * nz;
+  for (int k0 = lane; k0 < nz; k0 += 64) {
+    const int k1 = k0 + 32;
+    const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
+    const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+    if (x0 == 0.0f && x1 == 0.0f) continue;
+    UPair up;
+    voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+    if (x0 == 0.0f) up.n0 = 0;
+    if (x1 == 0.0f) up.n1 = 0;
+    const int L = max(up.n0, up.n1);
+    if (L <= 0) continue;
+    const float2 xr = mul2(make_float2(x0, x1), up.rho);
+    float2 Fp = cubic_prim2(up.start);
+    float2 lf = f2(1.0f);
+    for (int l = 0; l < L; ++l) {
+      const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+      const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
+      if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
+      if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
+      Fp = F;
+      lf = add2(lf, f2(1.0f));
+    }
+    if (up.n0 > 0) {
+      lo = min(lo, up.lo0);
+      hi = max(hi, up.lo0 + up.n0);
+    }
+    if (up.n1 > 0) {
+      lo = min(lo, up.lo1);
+      hi = max(hi, up.lo1 + up.n1);
+    }
+  }
+  lo_out = __reduce_min_sync(FULLM, lo);
+  hi_out = __reduce_max_sync(FULLM, hi);
+}
+
+// ---------------------------------------------------------------------------
+// Direct projector, column pairs.  Same band decomposition as
+// k_fwd3d_band_fast, but a warp takes the hits of a chunk two at a time
+// (neighbouring columns along x, whose footprints nearly coincide), builds
+// both profiles and spreads w1(r) P1[u] + w2(r) P2[u] over the union of
+// their rows and cells: one shared-memory atomic per cell of the union
+// instead of one per cell of each column.
+// ---------------------------------------------------------------------------
+template <int GEOM>
+__global__ void __launch_bounds__(512)
+k_fwd3d_band_pair(const Params3D P, const View3D *__restrict__ views,
+                  const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
+                  long sino_view_stride, int band_rows, int *__restrict__ err)
+{
+  extern __shared__ float sm[];
+  __shared__ View3D sV;
+  __shared__ int s_next;
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nu = P.nu, nv = P.nv;
+  float *acc = sm;
+  float *prof1 = sm + band_rows * nu + warp * 2 * nu;
+  float *prof2 = prof1 + nu;
+  float *wv1 = sm + band_rows * nu + nwarps * 2 * nu + warp * 2 * band_rows;
+  float *wv2 = wv1 + band_rows;
+  const int vi = blockIdx.y;
+  if (threadIdx.x < (int)(sizeof(View3D) / 8))
+    reinterpret_cast<double *>(&sV)[threadIdx.x] =
+        reinterpret_cast<const double *>(views + vi)[threadIdx.x];
+  if (threadIdx.x == 0) s_next = 0;
+  const int v0 = blockIdx.x * band_rows;
+  const int v1 = min(v0 + band_rows, nv);
+  for (int t = threadIdx.x; t < band_rows * nu; t += blockDim.x) acc[t] = 0.f;
+  for (int t = lane; t < 2 * nu; t += 32) prof1[t] = 0.f;
+  for (int t = lane; t < 2 * band_rows; t += 32) wv1[t] = 0.f;
+  __syncthreads();
+  const View3D &V = sV;
+  const int ncols = P.nx * P.ny;
+  const int nchunks = (ncols + 31) >> 5;
+
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(&s_next, 1);
+    chunk = __shfl_sync(FULLM, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int mycol = (chunk << 5) + lane;
+    ColGeo<MODEL_CUBIC> c;
+    bool hit = false;
+    if (mycol < ncols) {
+      column_geo<GEOM, MODEL_CUBIC>(P, V, mycol % P.nx, mycol / P.nx, 0, c);
+      if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+      hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
+    }
+    unsigned mask = __ballot_sync(FULLM, hit);
+    while (mask) {
+      const int s1 = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int s2 = mask ? __ffs(mask) - 1 : -1;
+      if (s2 >= 0) mask &= mask - 1;
+      const ColGeo<MODEL_CUBIC> c1 = shfl_colc(c, s1);
+      const ColGeo<MODEL_CUBIC> c2 = shfl_colc(c, s2 >= 0 ? s2 : s1);
+      // rows of each column inside the band, and their union
+      const int rb1 = max(c1.vax.lo, v0), re1 = min(c1.vax.lo + c1.vax.n, v1);
+      int rb = rb1, re = re1, rb2 = 0, re2 = 0;
+      if (s2 >= 0) {
+        rb2 = max(c2.vax.lo, v0);
+        re2 = min(c2.vax.lo + c2.vax.n, v1);
+        rb = min(rb, rb2);
+        re = max(re, re2);
+      }
+      for (int r = rb + lane; r < re; r += 32) {
+        wv1[r - v0] = (r >= rb1 && r < re1) ? axis_weight<MODEL_CUBIC>(c1.vax, r - c1.vax.lo, P) : 0.f;
+        wv2[r - v0] = (s2 >= 0 && r >= rb2 && r < re2) ? axis_weight<MODEL_CUBIC>(c2.vax, r - c2.vax.lo, P) : 0.f;
+      }
+      int lo1, hi1, lo2 = INT_MAX, hi2 = INT_MIN;
+      column_profile<GEOM>(P, V, vol, gate_stride, c1, (chunk << 5) + s1, prof1, lane, lo1, hi1);
+      if (s2 >= 0) column_profile<GEOM>(P, V, vol, gate_stride, c2, (chunk << 5) + s2, prof2, lane, lo2, hi2);
+      const int lo = min(lo1, lo2), hi = max(hi1, hi2);
+      __syncwarp();
+      if (lo < hi) {
+        for (int r = rb; r < re; ++r) {
+          const float w1 = wv1[r - v0], w2 = wv2[r - v0];
+          float *row = acc + (r - v0) * nu;
+          for (int u = lo + lane; u < hi; u += 32) atomicAdd(row + u, fmaf(w2, prof2[u], w1 * prof1[u]));
+        }
+        __syncwarp();
+        for (int u = lo + lane; u < hi; u += 32) {
+          prof1[u] = 0.f;
+          prof2[u] = 0.f;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  float *out = sino + (long)vi * sino_view_stride;
+  const int nrow = v1 - v0;
+  for (int t = threadIdx.x; t < nrow * nu; t += blockDim.x) {
+    const int r = t / nu, u = t - r * nu;
+    out[(long)(v0 + r) * nu + u] += acc[t];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Direct projector, atomic-free band accumulation ("pull").
 //
@@ -492,6 +640,16 @@ static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
     if (L.P.nu <= 512) return fwd_pull<GEOM, 16>(L, st);
   }
   dim3 grid((L.P.nv + L.band_rows - 1) / L.band_rows, L.nviews);
+  if (L.cols == 2) {
+    const size_t smem = sizeof(float) * ((size_t)L.band_rows * L.P.nu + 2 * (size_t)L.warps * L.P.nu +
+                                         2 * (size_t)L.warps * L.band_rows);
+    auto kern = k_fwd3d_band_pair<GEOM>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, L.warps * 32, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino,
+                                          L.sino_view_stride, L.band_rows, L.err);
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(float) * ((size_t)L.band_rows * L.P.nu + (size_t)L.warps * L.P.nu +
                                        (size_t)L.warps * L.band_rows);
   auto kern = k_fwd3d_band_fast<GEOM>;

@@ -16,6 +16,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "kernels.h"
@@ -174,6 +175,31 @@ enum {
   kSlots = 128
 };
 
+// Work buffers are kept between calls with the same sizes (a reconstruction
+// loop over many samples then allocates once); released at exit.
+struct Workspace {
+  std::mutex mu;
+  int device = -1;
+  long n = 0, m = 0;
+  int mem = 0;
+  std::vector<float *> bufs;
+  double *acc = nullptr;
+  void release()
+  {
+    for (float *p : bufs) cudaFree(p);
+    bufs.clear();
+    if (acc) cudaFree(acc);
+    acc = nullptr;
+    n = m = 0;
+    mem = 0;
+  }
+};
+Workspace &workspace()
+{
+  static Workspace *ws = new Workspace;  // never destroyed: the CUDA context may be gone at exit
+  return *ws;
+}
+
 struct Solver {
   trtt_b200_plan3d *plan;
   cudaStream_t st;
@@ -181,26 +207,25 @@ struct Solver {
   long tx, ty, tz;  // dims handed to the TV / spline kernels (fastest first)
   const float *y, *w;
   double mu, eps;
-  std::vector<float *> bufs;
+  Workspace *ws = nullptr;
+  size_t next = 0;  // next buffer of the workspace to hand out
   bool oom = false;
   float *hx, *wr, *z, *tmp, *gz, *sg;
   long nviews;
   double *acc = nullptr;  // device scalars (kSlots)
 
+  // hand out the workspace's buffers in a fixed order; allocate on first use
   float *alloc(long count)
   {
+    if (next < ws->bufs.size()) return ws->bufs[next++];
     float *p = nullptr;
     if (cudaMalloc(&p, sizeof(float) * count) != cudaSuccess) {
       oom = true;
       return nullptr;
     }
-    bufs.push_back(p);
+    ws->bufs.push_back(p);
+    ++next;
     return p;
-  }
-  ~Solver()
-  {
-    for (float *p : bufs) cudaFree(p);
-    if (acc) cudaFree(acc);
   }
 
   // f(x) and g = grad f(x); f is read back (synchronises)
@@ -252,7 +277,25 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   };
 
+  Workspace &W = workspace();
+  std::lock_guard<std::mutex> lock(W.mu);
+  int dev = 0;
+  TRTT_CK(cudaGetDevice(&dev));
+  if (W.device != dev || W.n != nx * ny * nz || W.m != nviews * nu * nv || W.mem != mem) {
+    if (W.device >= 0 && W.device != dev) {  // free the other device's buffers there
+      TRTT_CK(cudaSetDevice(W.device));
+      W.release();
+      TRTT_CK(cudaSetDevice(dev));
+    } else {
+      W.release();
+    }
+    W.device = dev;
+    W.n = nx * ny * nz;
+    W.m = nviews * nu * nv;
+    W.mem = mem;
+  }
   Solver S;
+  S.ws = &W;
   S.plan = plan;
   S.st = static_cast<cudaStream_t>(stream);
   S.n = nx * ny * nz;
@@ -263,7 +306,8 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
   S.w = w;
   S.mu = mu;
   S.eps = eps;
-  TRTT_CK(cudaMalloc(&S.acc, sizeof(double) * kSlots));
+  if (!W.acc) TRTT_CK(cudaMalloc(&W.acc, sizeof(double) * kSlots));
+  S.acc = W.acc;
   const long n = S.n;
   S.hx = S.alloc(S.m);
   S.wr = S.alloc(S.m);
@@ -280,6 +324,7 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
   }
   if (S.oom) {
     cudaGetLastError();
+    W.release();
     return fail("recon3d: out of device memory");
   }
   cudaStream_t st = S.st;

@@ -87,9 +87,15 @@ class Projector3D:
                    "trtt_b200_plan3d_set_gates")
         self.nt = int(nt)
 
-    def set_tiles(self, band_rows: int = 0, warps: int = 0) -> None:
-        _lib.check(_lib.load().trtt_b200_plan3d_set_tiles(self._h, band_rows, warps),
+    def set_tiles(self, band_rows: int = 0, warps: int = 0, cols: int = 1) -> None:
+        """Direct-projector kernel shape: (band rows, warps) of the band kernel
+        ((0, 0): automatic; (-2, 0): atomic-free variant) and the number of
+        neighbouring columns spread together (1 or 2)."""
+        lib = _lib.load()
+        _lib.check(lib.trtt_b200_plan3d_set_columns(self._h, 1), "trtt_b200_plan3d_set_columns")
+        _lib.check(lib.trtt_b200_plan3d_set_tiles(self._h, band_rows, warps),
                    "trtt_b200_plan3d_set_tiles")
+        _lib.check(lib.trtt_b200_plan3d_set_columns(self._h, cols), "trtt_b200_plan3d_set_columns")
 
     @property
     def factorized(self) -> bool:
@@ -152,13 +158,15 @@ class Projector3D:
         raise ValueError("unsupported job (0 = direct, 1 = transpose)")
 
     # -- tuning and graph capture ----------------------------------------------
-    TILE_CANDIDATES = [(0, 0), (16, 16), (24, 16), (32, 8), (32, 12), (48, 8), (-2, 0)]
+    TILE_CANDIDATES = [(0, 0), (16, 16), (24, 16), (32, 8), (32, 12), (48, 8), (-2, 0),
+                       (0, 0, 2), (32, 16, 2), (32, 8, 2), (24, 8, 2), (16, 16, 2)]
 
     def autotune(self, vol=None, layout="columns", candidates=None, reps=2, nview=None):
-        """Time the direct projector with each candidate (band_rows, warps)
-        setting (see trtt_b200_plan3d_set_tiles; (-2, 0) is the atomic-free
-        band kernel) on `vol` (random data of the plan's volume shape if
-        None) and keep the fastest.  Returns {candidate: ms} and the choice."""
+        """Time the direct projector with each candidate (band_rows, warps[,
+        cols]) setting (see set_tiles; (-2, 0) is the atomic-free band
+        kernel, cols = 2 the column-pair kernel) on `vol` (random data of the
+        plan's volume shape if None) and keep the fastest.  Returns
+        {candidate: ms} and the choice."""
         torch = _torch()
         if vol is None:
             vol = torch.rand(self.volume_shape(layout), device=self.device)

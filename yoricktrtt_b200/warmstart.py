@@ -140,13 +140,15 @@ def train(net, pairs, epochs=10, batch=2, lr=1e-3, lr_final=1e-4, seed=0, log=No
     """Adam with a cosine learning-rate schedule and random flips; returns
     the per-epoch mean losses and the training time.
 
-    obj_weight > 0 adds the term obj_weight (f(max(out, 0)) - f_target) /
-    f_target to the MSE loss, f the sample's own TV objective (the cost the
-    warm-started iteration will minimise): its gradient, the objective
-    gradient at the network output, reaches the network through
+    obj_weight > 0 adds the term obj_weight log(f(max(out, 0)) / f_target)
+    to the MSE loss, f the sample's own TV objective (the cost the
+    warm-started iteration will minimise; f_target, the objective of the
+    target, is its minimum up to the target's convergence): its gradient
+    grad f / f at the network output reaches the network through
     ``extra_grad``.  Low-frequency errors, which dominate the data term and
     which the mean squared error weighs no more than any other, are then
-    penalised by what they cost the iteration."""
+    penalised by what they cost the iteration; dividing by f (the log)
+    keeps the term bounded while f is still far above its minimum."""
     torch = _torch()
     inputs, targets = pairs.inputs, pairs.targets
     N = inputs.shape[0]
@@ -181,8 +183,8 @@ def train(net, pairs, epochs=10, batch=2, lr=1e-3, lr_final=1e-4, seed=0, log=No
                 for j, i in enumerate(idx):
                     xh = torch.flip(out[j], back) if back else out[j]
                     obj.y, obj.w = problem.data(pairs.counts[int(i)])
-                    _, g = obj(xh.clamp(min=0.0).contiguous())
-                    g = g * (xh > 0) * (obj_weight / float(pairs.f_target[int(i)]))
+                    fv, g = obj(xh.clamp(min=0.0).contiguous())
+                    g = g * (xh > 0) * (obj_weight / fv)
                     extra[j] = torch.flip(g, back) if back else g
             acc += float(net.train_step(xb, tb, extra_grad=extra))
             step += 1
@@ -193,21 +195,28 @@ def train(net, pairs, epochs=10, batch=2, lr=1e-3, lr_final=1e-4, seed=0, log=No
     return losses, time.perf_counter() - t0
 
 
-def _hit_time(info, f_star, rtol=1e-6):
-    """Wall time of the first iterate with f <= f_star + rtol |f_star|."""
-    lim = f_star + rtol * abs(f_star)
-    for f, t in zip(info.f, info.times):
+def _hit(info, f_ref, rtol):
+    """(iteration, wall time) of the first iterate with f <= f_ref (1 + rtol)."""
+    lim = f_ref + rtol * abs(f_ref)
+    for k, (f, t) in enumerate(zip(info.f, info.times)):
         if f <= lim:
-            return t
-    return None
+            return k, t
+    return None, None
 
 
-def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, log=None):
+TOLS = (1e-4, 1e-5, 1e-6)
+
+
+def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, ref_maxiter=600, log=None):
     """Per held-out seed: the plain method from zero, from the normalised
     backprojection and from each network's output (``nets``: a network or
-    {name: network}), to the same stopping rule.  Times are wall clock (the
-    iteration reads FP64 scalars back every step) and include building the
-    start (backprojection, network inference)."""
+    {name: network}), each to the stopping rule |f_k - f_k+1| <= frtol
+    max(|f_k|, |f_k+1|).  A reference run from zero without the stopping
+    rule (ref_maxiter iterations) gives f_ref, the lowest objective reached;
+    for every start the iterations and wall time to f <= f_ref (1 + tol) are
+    reported for tol in TOLS.  Times are wall clock (the iteration reads FP64
+    scalars back every step) and include building the start
+    (backprojection, network inference)."""
     torch = _torch()
     if not isinstance(nets, dict):
         nets = {"learned": nets}
@@ -215,13 +224,12 @@ def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, log=None):
     for s in seeds:
         _, y, w = problem.sample(s)
         res = {"seed": int(s)}
+        runs = {}
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         x0, info0 = problem.reconstruct(y, w, frtol=frtol, maxiter=maxiter)
         torch.cuda.synchronize()
-        res["zero"] = {"seconds": time.perf_counter() - t0, "iterations": info0.iterations,
-                       "evaluations": info0.evaluations, "f": info0.f[-1], "converged": info0.converged}
-        f_star = info0.f[-1]
+        runs["zero"] = (time.perf_counter() - t0, 0.0, x0, info0)
         for name in ["backprojection"] + list(nets):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -232,38 +240,57 @@ def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, log=None):
             t_start = time.perf_counter() - t0
             x, info = problem.reconstruct(y, w, x0=start, frtol=frtol, maxiter=maxiter)
             torch.cuda.synchronize()
-            hit = _hit_time(info, f_star)
-            res[name] = {"seconds": time.perf_counter() - t0, "start_seconds": t_start,
-                         "iterations": info.iterations, "evaluations": info.evaluations,
-                         "f": info.f[-1], "f_start": info.f[0], "converged": info.converged,
-                         "seconds_to_plain_f": None if hit is None else t_start + hit,
-                         "rel_diff_vs_plain": float(torch.linalg.norm(x - x0) / torch.linalg.norm(x0))}
+            runs[name] = (time.perf_counter() - t0, t_start, x, info)
+        _, info_ref = problem.reconstruct(y, w, frtol=0.0, maxiter=ref_maxiter)
+        f_ref = min([info_ref.f[-1]] + [r[3].f[-1] for r in runs.values()])
+        res["f_ref"] = f_ref
+        for name, (sec, t_start, x, info) in runs.items():
+            d = {"seconds": sec, "start_seconds": t_start, "iterations": info.iterations,
+                 "evaluations": info.evaluations, "f": info.f[-1], "f_start": info.f[0],
+                 "converged": info.converged,
+                 "rel_diff_vs_zero": float(torch.linalg.norm(x - x0) / torch.linalg.norm(x0))}
+            for tol in TOLS:
+                k, t = _hit(info, f_ref, tol)
+                d[f"to_{tol:g}"] = None if k is None else {"iterations": k, "seconds": t_start + t}
+            res[name] = d
         rows.append(res)
         if log:
-            log(f"seed {s}: " + ", ".join(f"{k} {res[k]['seconds']:.2f} s ({res[k]['iterations']} it)"
-                                          for k in ["zero", "backprojection"] + list(nets)))
+            log(f"seed {s}: " + ", ".join(
+                f"{k} {res[k]['iterations']} it / {res[k]['seconds']:.2f} s"
+                f" (1e-5: {res[k]['to_1e-05']['iterations'] if res[k]['to_1e-05'] else '-'} it)"
+                for k in runs))
     problem.pr.status()
     return rows
 
 
 def summarize(rows):
     out = {}
-    names = [k for k in rows[0] if k != "seed"]
+    names = [k for k in rows[0] if k not in ("seed", "f_ref")]
     for name in names:
         sec = [r[name]["seconds"] for r in rows]
         it = [r[name]["iterations"] for r in rows]
-        out[name] = {"seconds_mean": float(np.mean(sec)), "seconds_median": float(np.median(sec)),
-                     "iterations_mean": float(np.mean(it)),
-                     "converged": int(sum(bool(r[name]["converged"]) for r in rows))}
-        if name != "zero":
-            hits = [r[name]["seconds_to_plain_f"] for r in rows]
+        o = {"stop_rule": {"seconds_mean": float(np.mean(sec)), "seconds_median": float(np.median(sec)),
+                           "iterations_mean": float(np.mean(it)),
+                           "converged": int(sum(bool(r[name]["converged"]) for r in rows)),
+                           "final_f_rel_excess_mean": float(np.mean(
+                               [(r[name]["f"] - r["f_ref"]) / abs(r["f_ref"]) for r in rows]))}}
+        for tol in TOLS:
+            hits = [r[name][f"to_{tol:g}"] for r in rows]
             ok = [h for h in hits if h is not None]
-            out[name]["reached_plain_f"] = len(ok)
-            out[name]["seconds_to_plain_f_median"] = float(np.median(ok)) if ok else None
-            f_rel = [(r[name]["f"] - r["zero"]["f"]) / abs(r["zero"]["f"]) for r in rows]
-            out[name]["final_f_rel_vs_zero_mean"] = float(np.mean(f_rel))
-    z = out["zero"]["seconds_mean"]
+            o[f"to_{tol:g}"] = {"reached": len(ok),
+                                "iterations_median": float(np.median([h["iterations"] for h in ok])) if ok else None,
+                                "seconds_median": float(np.median([h["seconds"] for h in ok])) if ok else None}
+        out[name] = o
+    z = out["zero"]
     for name in names:
-        if name != "zero":
-            out[name]["speedup_vs_zero"] = z / out[name]["seconds_mean"]
+        if name == "zero":
+            continue
+        o = out[name]
+        o["speedup_vs_zero"] = {"stop_rule_seconds_mean": z["stop_rule"]["seconds_mean"] /
+                                o["stop_rule"]["seconds_mean"]}
+        for tol in TOLS:
+            k = f"to_{tol:g}"
+            if z[k]["iterations_median"] and o[k]["iterations_median"]:
+                o["speedup_vs_zero"][k + "_iterations_median"] = z[k]["iterations_median"] / max(
+                    1.0, o[k]["iterations_median"])
     return out
