@@ -211,8 +211,9 @@ def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, ref_maxiter
     """Per held-out seed: the plain method from zero, from the normalised
     backprojection and from each network's output (``nets``: a network or
     {name: network}), each to the stopping rule |f_k - f_k+1| <= frtol
-    max(|f_k|, |f_k+1|).  A reference run from zero without the stopping
-    rule (ref_maxiter iterations) gives f_ref, the lowest objective reached;
+    max(|f_k|, |f_k+1|).  f_ref is the lowest objective reached by these
+    runs and, if ref_maxiter > 0, by a reference run from zero without the
+    stopping rule (ref_maxiter iterations);
     for every start the iterations and wall time to f <= f_ref (1 + tol) are
     reported for tol in TOLS.  Times are wall clock (the iteration reads FP64
     scalars back every step) and include building the start
@@ -241,8 +242,10 @@ def evaluate(problem: Problem, nets, seeds, frtol=1e-6, maxiter=500, ref_maxiter
             x, info = problem.reconstruct(y, w, x0=start, frtol=frtol, maxiter=maxiter)
             torch.cuda.synchronize()
             runs[name] = (time.perf_counter() - t0, t_start, x, info)
-        _, info_ref = problem.reconstruct(y, w, frtol=0.0, maxiter=ref_maxiter)
-        f_ref = min([info_ref.f[-1]] + [r[3].f[-1] for r in runs.values()])
+        f_ref = min(r[3].f[-1] for r in runs.values())
+        if ref_maxiter > 0:
+            _, info_ref = problem.reconstruct(y, w, frtol=0.0, maxiter=ref_maxiter)
+            f_ref = min(f_ref, info_ref.f[-1])
         res["f_ref"] = f_ref
         for name, (sec, t_start, x, info) in runs.items():
             d = {"seconds": sec, "start_seconds": t_start, "iterations": info.iterations,

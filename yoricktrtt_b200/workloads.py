@@ -231,7 +231,8 @@ def _log(msg):
 
 
 def learned_warmstart(n_train=400, n_test=20, epochs=8, batch=2, lr=1e-3, target_maxiter=150,
-                      eval_maxiter=500, obj_weight=0.0, compare=False, weights=None, seed=0):
+                      eval_maxiter=500, ref_maxiter=600, obj_weight=0.0, compare=False, weights=None,
+                      seed=0):
     """compare=True trains two networks from the same initialisation, with
     the mean squared error alone and with the objective term of
     warmstart.train (obj_weight), and evaluates both."""
@@ -256,7 +257,7 @@ def learned_warmstart(n_train=400, n_test=20, epochs=8, batch=2, lr=1e-3, target
             net.save(weights if len(variants) == 1 else weights.replace(".npz", f"_{name}.npz"))
     del pairs
     torch.cuda.empty_cache()
-    rows = evaluate(pb, nets, test_seeds, maxiter=eval_maxiter, log=_log)
+    rows = evaluate(pb, nets, test_seeds, maxiter=eval_maxiter, ref_maxiter=ref_maxiter, log=_log)
     return {"config": f"learned warm start: 128^3 ellipsoid phantoms, 90 cone-beam views on 256^2, "
                       f"Poisson I0=1e4, VMLM-B + TV (mu={pb.mu:g}, eps={pb.eps:g}); {n_train} training "
                       f"pairs (targets: VMLM-B from zero, at most {target_maxiter} iterations or 1e-6), "
@@ -266,7 +267,7 @@ def learned_warmstart(n_train=400, n_test=20, epochs=8, batch=2, lr=1e-3, target
             "summary": summarize(rows), "per_seed": rows}
 
 
-def learned_eval(weights=None, n_test=20, eval_maxiter=500, seed=0):
+def learned_eval(weights=None, n_test=20, eval_maxiter=500, ref_maxiter=600, seed=0):
     import os
     from .unet import UNet3D
     from .warmstart import Problem, evaluate, summarize
@@ -275,7 +276,7 @@ def learned_eval(weights=None, n_test=20, eval_maxiter=500, seed=0):
     net = UNet3D.load(weights)
     pb = Problem()
     test_seeds = list(range(seed + 20000, seed + 20000 + n_test))
-    rows = evaluate(pb, net, test_seeds, maxiter=eval_maxiter, log=_log)
+    rows = evaluate(pb, net, test_seeds, maxiter=eval_maxiter, ref_maxiter=ref_maxiter, log=_log)
     return {"config": f"learned warm start evaluation ({os.path.basename(weights)}): {n_test} held-out "
                       f"seeds, 128^3, 90 views, 256^2, Poisson I0=1e4, VMLM-B + TV to 1e-6",
             "summary": summarize(rows), "per_seed": rows}
