@@ -354,10 +354,11 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
       tc::fence_after_sync();
       const int buf = it % nstg;
       const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
-      for (int j = 0; j < 3; ++j) {
+      // the three accumulators alternate so that consecutive MMAs are independent
 #pragma unroll
-        for (int ks = 0; ks < KT / 16; ++ks) {
-          const uint64_t ad = tc::sdesc(as + (uint32_t)(ks * 256), 128u, (uint32_t)a.csa);
+      for (int ks = 0; ks < KT / 16; ++ks) {
+        const uint64_t ad = tc::sdesc(as + (uint32_t)(ks * 256), 128u, (uint32_t)a.csa);
+        for (int j = 0; j < 3; ++j) {
           const uint64_t bd = tc::sdesc(bs + (uint32_t)((ks * 16 + j) * 16), 128u, (uint32_t)a.csb);
           tc::mma_bf16(tmem + (uint32_t)(j * cin), ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
         }
