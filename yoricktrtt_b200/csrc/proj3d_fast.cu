@@ -494,7 +494,6 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
   const int col = blockIdx.x * nwarps + warp;
   if (col >= ncols) return;
   float *Q = sm + warp * nu;
-  float *wv = sm + nwarps * nu + warp * 64;
   const int i = col % P.nx, j = col / P.nx;
   const int kbase = blockIdx.y * (64 * KP);
   const int gate = blockIdx.z;
@@ -667,7 +666,7 @@ static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
   const int warps = 8;
   const int ncols = L.P.nx * L.P.ny;
   dim3 grid((ncols + warps - 1) / warps, (L.P.nz + 64 * KP - 1) / (64 * KP), L.ngates);
-  const size_t smem = sizeof(float) * ((size_t)warps * L.P.nu + (size_t)warps * 64);
+  const size_t smem = sizeof(float) * (size_t)warps * L.P.nu;
   auto kern = k_back3d_col_fast<GEOM, KP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

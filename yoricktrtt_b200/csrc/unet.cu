@@ -266,7 +266,6 @@ __global__ void __launch_bounds__(128) k_conv3_fwd(const FwdArgs a)
 // ---------------------------------------------------------------------------
 // weight gradient
 // ---------------------------------------------------------------------------
-constexpr int KT = 128;  // rows (K) per stage
 
 struct WgradArgs {
   const bf16 *dy;       // [rows][cout]
@@ -275,7 +274,8 @@ struct WgradArgs {
   float *part;          // [chunks][cout][27][cin]
   Grid3 g;
   long r0, r1;          // rows summed over
-  int steps;            // KT-row stages per CTA
+  int kt;               // rows (K) per stage: 128 or 256
+  int steps;            // kt-row stages per CTA
   int csa, csb, a_bytes, stage_bytes, nstg;
   uint32_t tmem_cols;
 };
@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int gidx = blockIdx.x, dzi = gidx / 3, dyi = gidx - 3 * (gidx / 3);
   const long off = (long)(dzi - 1) * a.g.plane + (long)(dyi - 1) * a.g.wp;
+  const int KT = a.kt;
   const long qbeg = a.r0 + (long)blockIdx.y * a.steps * KT;
   long rem = a.r1 - qbeg;
   int T = rem <= 0 ? 0 : (int)((rem + KT - 1) / KT);
@@ -300,12 +301,10 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
     for (int i = 0; i < nstg; ++i) tc::mbar_init(&mbar[i], 1);
     tc::mbar_fence_init();
   }
-  // zero the A chunks beyond cout once (the M = 64 MMAs read 8 chunks)
-  for (int b = 0; b < nstg; ++b) {
-    uint4 *z = reinterpret_cast<uint4 *>(smem + b * a.stage_bytes + nca * a.csa);
-    const int cnt = (8 - nca) * a.csa / 16;
-    for (int e = tid; e < cnt; e += 128) z[e] = make_uint4(0, 0, 0, 0);
-  }
+  // Only the cout/8 real chunks of the A operand are staged; the M = 64
+  // MMAs read the rows above cout from whatever follows them in shared
+  // memory (inside the allocation, which has a tail for the last stage):
+  // those accumulator rows are never read back.
   if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
   tc::fence_before_sync();
   __syncthreads();
@@ -355,7 +354,7 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
       const int buf = it % nstg;
       const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
       // the three accumulators alternate so that consecutive MMAs are independent
-#pragma unroll
+#pragma unroll 4
       for (int ks = 0; ks < KT / 16; ++ks) {
         const uint64_t ad = tc::sdesc(as + (uint32_t)(ks * 256), 128u, (uint32_t)a.csa);
         for (int j = 0; j < 3; ++j) {
@@ -705,6 +704,45 @@ int residency_smem(int smem, uint32_t tmem_cols)
   return smem < need ? need : smem;
 }
 
+// Stage layout of the weight-gradient kernel: 256 rows per stage when two
+// CTAs still fit on an SM, else 128; row ranges split into chunks so that
+// the grid (9 x chunks) covers the GPU about four times.
+struct WgradPlan {
+  int kt, csa, csb, a_bytes, stage_bytes, nstg, smem;
+  long chunks, steps;
+  uint32_t tmem_cols;
+};
+
+WgradPlan wgrad_plan(int cout, int cin, const Grid3 &g)
+{
+  WgradPlan p;
+  const int nca = cout / 8, ncb = cin / 8;
+  const int pad_a = nca == 2 ? 64 : nca == 4 ? 32 : 16;
+  const int pad_b = ncb == 2 ? 64 : ncb == 4 ? 32 : 16;
+  p.tmem_cols = pow2_cols(3 * cin);
+  for (int kt = 256; kt >= 128; kt /= 2) {
+    p.kt = kt;
+    p.csa = kt * 16 + pad_a;
+    p.csb = (((kt + 2) * 16 + 127) / 128) * 128 + pad_b;
+    p.a_bytes = ((nca * p.csa + 127) / 128) * 128;
+    p.stage_bytes = ((p.a_bytes + ncb * p.csb + 1023) / 1024) * 1024;
+    p.nstg = 4 * p.stage_bytes <= 112 * 1024 ? 4 : 3;
+    // tail: the last stage's MMAs read 8 chunk strides of A rows
+    const int tail = (((8 - nca) * p.csa + 127) / 128) * 128;
+    p.smem = residency_smem(p.nstg * p.stage_bytes + tail, p.tmem_cols);
+    if (p.smem <= 112 * 1024) break;
+  }
+  const long total = (g.rows - 2 * g.plane + p.kt - 1) / p.kt;
+  long chunks = 592 / 9;
+  if (chunks > total) chunks = total;
+  if (chunks < 1) chunks = 1;
+  p.steps = (total + chunks - 1) / chunks;
+  if (p.steps < 1) p.steps = 1;
+  p.chunks = (total + p.steps - 1) / p.steps;
+  if (p.chunks < 1) p.chunks = 1;
+  return p;
+}
+
 template <typename K>
 cudaError_t set_smem(K kern, int bytes)
 {
@@ -762,14 +800,9 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
 
 size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w)
 {
-  if (!grid_ok(nb, d, h, w) || cout <= 0 || cin <= 0) return 0;
-  const Grid3 g = make_grid(nb, d, h, w);
-  const long total = (g.rows - 2 * g.plane + KT - 1) / KT;
-  long chunks = 592 / 9;
-  if (chunks > total) chunks = total;
-  const long steps = (total + chunks - 1) / chunks;
-  chunks = (total + steps - 1) / steps;
-  return (size_t)chunks * cout * 27 * cin * sizeof(float);
+  if (!grid_ok(nb, d, h, w) || cout <= 0 || cin <= 0 || cout % 8 || cin % 8) return 0;
+  WgradPlan p = wgrad_plan(cout, cin, make_grid(nb, d, h, w));
+  return (size_t)p.chunks * cout * 27 * cin * sizeof(float);
 }
 
 int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2, float *dw,
@@ -792,26 +825,21 @@ int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, cons
   a.g = make_grid(nb, d, h, w);
   a.r0 = a.g.plane;
   a.r1 = a.g.rows - a.g.plane;
-  const long total = (a.r1 - a.r0 + KT - 1) / KT;
-  long chunks = 592 / 9;
-  if (chunks > total) chunks = total;
-  const long steps = (total + chunks - 1) / chunks;
-  chunks = (total + steps - 1) / steps;
-  if (steps > 0x7FFFFFFFL) return fail("conv3_wgrad: too many rows");
-  a.steps = (int)steps;
+  const WgradPlan pl = wgrad_plan(cout, cin, a.g);
+  if (pl.steps > 0x7FFFFFFFL) return fail("conv3_wgrad: too many rows");
+  const long chunks = pl.chunks;
+  a.kt = pl.kt;
+  a.steps = (int)pl.steps;
   const size_t need = (size_t)chunks * cout * 27 * cin * sizeof(float);
   if (scratch_bytes < need) return fail("conv3_wgrad: scratch too small");
   a.part = static_cast<float *>(scratch);
-  const int nca = cout / 8, ncb = cin / 8;
-  const int pad_a = nca == 2 ? 64 : nca == 4 ? 32 : 16;
-  const int pad_b = ncb == 2 ? 64 : ncb == 4 ? 32 : 16;
-  a.csa = KT * 16 + pad_a;
-  a.csb = (((KT + 2) * 16 + 127) / 128) * 128 + pad_b;
-  a.a_bytes = ((8 * a.csa + 127) / 128) * 128;
-  a.stage_bytes = ((a.a_bytes + ncb * a.csb + 1023) / 1024) * 1024;
-  a.nstg = 4 * a.stage_bytes <= 112 * 1024 ? 4 : 3;
-  a.tmem_cols = pow2_cols(3 * cin);
-  int smem = residency_smem(a.nstg * a.stage_bytes, a.tmem_cols);
+  a.csa = pl.csa;
+  a.csb = pl.csb;
+  a.a_bytes = pl.a_bytes;
+  a.stage_bytes = pl.stage_bytes;
+  a.nstg = pl.nstg;
+  a.tmem_cols = pl.tmem_cols;
+  const int smem = pl.smem;
   if (smem > 227 * 1024) return fail("conv3_wgrad: stage too large");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TRTT_CK(set_smem(k_conv3_wgrad, smem));
