@@ -54,7 +54,7 @@ __device__ __forceinline__ void voxel_u_pair(const Params3D &P, const View3D &V,
     const float2 du2 = fma2(mul2(uca, uca), f2(c.inv_den), f2(1.0f));
     const float2 dlt = mul2(du2, make_float2(rsqrtf(du2.x), rsqrtf(du2.y)));
     const float2 h = mul2(dlt, f2(c.h_u0m));
-    scl = make_float2(__frcp_rn(h.x), __frcp_rn(h.y));
+    scl = make_float2(__fdividef(1.0f, h.x), __fdividef(1.0f, h.y));  // 2 ulp, h in (0, 2^126)
     hs = mul2(h, f2((float)P.hs0));
     up.rho = mul2(dlt, f2(c.rho0c));
   } else {

@@ -17,6 +17,7 @@
 namespace trtt {
 
 static constexpr unsigned FULLM = 0xffffffffu;
+static constexpr int SPREAD_CHUNKS = 16;  // footprints up to 512 cells wide spread from registers
 
 __device__ __forceinline__ ColGeo<MODEL_CUBIC> shfl_colc(const ColGeo<MODEL_CUBIC> &c, int src)
 {
@@ -132,7 +133,29 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
       lo = __reduce_min_sync(FULLM, lo);
       hi = __reduce_max_sync(FULLM, hi);
       __syncwarp();
-      if (lo < hi) {
+      if (lo < hi && hi - lo <= 32 * SPREAD_CHUNKS) {
+        // profile read once into registers (and cleared), then one shared
+        // atomic per (row, cell) of the footprint
+        float pv[SPREAD_CHUNKS];
+#pragma unroll
+        for (int c = 0; c < SPREAD_CHUNKS; ++c) {
+          const int u = lo + lane + 32 * c;
+          pv[c] = 0.f;
+          if (u < hi) {
+            pv[c] = prof[u];
+            prof[u] = 0.f;
+          }
+        }
+        for (int r = 0; r < nr; ++r) {
+          const float w = wv[r];
+          float *row = acc + (rb - v0 + r) * nu;
+#pragma unroll
+          for (int c = 0; c < SPREAD_CHUNKS; ++c) {
+            const int u = lo + lane + 32 * c;
+            if (u < hi) atomicAdd(row + u, w * pv[c]);
+          }
+        }
+      } else if (lo < hi) {
         for (int r = 0; r < nr; ++r) {
           const float w = wv[r];
           float *row = acc + (rb - v0 + r) * nu;
