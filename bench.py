@@ -339,8 +339,9 @@ def run_e2e(sc, vol_h, args, dev):
     from yoricktrtt_b200 import _lib
     lib = _lib.load()
     vol64 = torch.from_numpy(np.ascontiguousarray(vol_h, dtype=np.float64)).pin_memory().numpy()
-    det = torch.zeros((VIEWS, ND, ND), dtype=torch.float64).pin_memory().numpy()
-    back = torch.zeros((N, N, N), dtype=torch.float64).pin_memory().numpy()
+    det_t = torch.zeros((VIEWS, ND, ND), dtype=torch.float64).pin_memory()
+    back_t = torch.zeros((N, N, N), dtype=torch.float64).pin_memory()
+    det, back = det_t.numpy(), back_t.numpy()  # same memory, for the C call
     xos = np.ascontiguousarray(sc.xos)
     xsd = np.ascontiguousarray(sc.xsd)
 
@@ -351,8 +352,10 @@ def run_e2e(sc, vol_h, args, dev):
         _lib.check(rc, "trtt_b200_cb3d_batch")
 
     def step():
-        det.fill(0.0)
-        back.fill(0.0)
+        # the caller zeroes the outputs (the plugin accumulates into them);
+        # torch's fill uses the host threads
+        det_t.zero_()
+        back_t.zero_()
         call(det, vol64, 0)
         call(back, det, 1)
 

@@ -242,6 +242,28 @@ def test_batch_entry_point(oracle_port):
         assert rel_l2(out[v], ref) <= TOL
 
 
+def test_batch_entry_point_transpose_chunks(oracle_port):
+    """Transpose through the host-buffer batch call: the detector stack is
+    uploaded and projected back in view chunks; accumulate onto a non-zero
+    output, twice in a row."""
+    from yoricktrtt_b200 import _lib
+    sc = _scan(G.TRTT_CONE_BEAM, views=13)
+    rng = np.random.default_rng(5)
+    det = rng.random((sc.nviews, sc.nv, sc.nu))
+    lib = _lib.load()
+    ref = np.zeros((sc.nz, sc.ny, sc.nx))
+    for v in range(sc.nviews):
+        oracle_port.cb3d(ref, np.ascontiguousarray(det[v]), sc, v, 1)
+    out = np.full((sc.nz, sc.ny, sc.nx), 0.5)
+    for call in range(2):
+        rc = lib.trtt_b200_cb3d_batch(
+            _lib.dptr(out), _lib.dptr(det), sc.nx, sc.ny, sc.nz, sc.s_scl, sc.s_deg, None, 0,
+            1.0, None, sc.nu, sc.nv, sc.u_scl, sc.v_scl, sc.nviews,
+            _lib.dptr(np.ascontiguousarray(sc.xos)), _lib.dptr(np.ascontiguousarray(sc.xsd)), 4, 1)
+        assert rc == 0, _lib.last_error()
+        assert rel_l2(out - 0.5, (call + 1) * ref) <= TOL
+
+
 @pytest.mark.parametrize("model", ["cubic", "table"])
 def test_4d_gates(oracle_port, model):
     """Per-gate projection of the 4D path: view k sees

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "host3d.h"
@@ -357,10 +358,19 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   TRTT_CK(D.err.ensure(sizeof(int)));
   TRTT_CK(cudaMemsetAsync(D.err.p, 0, sizeof(int), st));
   TRTT_CK(D.in64.ensure(sizeof(double) * nin));
-  TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+  TRTT_CK(D.out64.ensure(sizeof(double) * nout));
   TRTT_CK(D.vol32.ensure(sizeof(float) * nvox));
   TRTT_CK(D.det32.ensure(sizeof(float) * npix));
+  cudaStream_t cp = D.copy;
+  // The copy stream brings `out` to the device while the kernels run (it is
+  // only read there: the host array is written after the error check).
+  // It must not start before the previous call's read-back of out64 is done.
+  TRTT_CK(cudaEventRecord(D.ev[0], st));
+  TRTT_CK(cudaStreamWaitEvent(cp, D.ev[0], 0));
   if (job == 0) {
+    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(cudaEventRecord(D.ev[1], cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
     Fwd3DLaunch L;
@@ -379,7 +389,6 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     TRTT_CK(launch_fwd3d(L, st));
     count_launch(2);
   } else {
-    TRTT_CK(f64_to_f32(D.in64.as<double>(), D.det32.as<float>(), npix, st));
     TRTT_CK(cudaMemsetAsync(D.vol32.p, 0, sizeof(float) * nvox, st));
     std::vector<int> gp = {0, (int)nviews};
     std::vector<GateEntry> ge(nviews);
@@ -395,17 +404,33 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     L.gate_ptr = gp_dev;
     L.entries = ge_dev;
     L.ngates = 1;
-    L.view_lo = 0;
-    L.view_hi = (int)nviews;
-    L.sino = D.det32.as<float>();
     L.sino_view_stride = nu * nv;
     L.vol = D.vol32.as<float>();
     L.gate_stride = nvox;
     L.factorized = fact ? 1 : 0;
     L.err = D.err.as<int>();
-    TRTT_CK(launch_back3d(L, st));
-    count_launch(2);
+    // the detector stack arrives in (at most 6) view chunks on the copy
+    // stream; each chunk is projected back (accumulating into the volume)
+    // as soon as it is on the device, while the next chunk is copied
+    const int nchunk = (int)std::min<long>(nviews, 6);
+    const int per = (int)((nviews + nchunk - 1) / nchunk);
+    for (int c = 0; c * per < nviews; ++c) {
+      const long v0 = (long)c * per, v1 = std::min<long>(nviews, v0 + per);
+      const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
+      TRTT_CK(cudaMemcpyAsync(D.in64.as<double>() + off, in + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, cp));
+      TRTT_CK(f64_to_f32(D.in64.as<double>() + off, D.det32.as<float>() + off, cnt, cp));
+      TRTT_CK(cudaEventRecord(D.ev[2 + c], cp));
+      TRTT_CK(cudaStreamWaitEvent(st, D.ev[2 + c], 0));
+      L.view_lo = (int)v0;
+      L.view_hi = (int)v1;
+      L.sino = D.det32.as<float>() + off;  // the kernel reads sino[view - view_lo]
+      TRTT_CK(launch_back3d(L, st));
+      count_launch(2);
+    }
+    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(cudaEventRecord(D.ev[1], cp));
   }
+  TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
   int herr = 0;
   TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   TRTT_CK(cudaStreamSynchronize(st));
@@ -413,9 +438,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
     return fail("a voxel lies in the source plane (wk == 0)");
   }
-  // out += result (FP64 accumulation on the device)
-  TRTT_CK(D.out64.ensure(sizeof(double) * nout));
-  TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, st));
+  // out += result (FP64 accumulation on the device; out64 holds out already)
   if (job == 0) {
     TRTT_CK(f32_add_to_f64(D.det32.as<float>(), D.out64.as<double>(), npix, st));
   } else {

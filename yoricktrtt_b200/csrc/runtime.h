@@ -37,6 +37,9 @@ struct DropIn {
   bool ready = false;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy = nullptr;  // host<->device copies that overlap the kernels
+  static constexpr int kEvents = 33;
+  cudaEvent_t ev[kEvents] = {};
   DevBuf in64, out64, vol32, det32, geom, gates, aux, err;
   cudaError_t init();
 };
