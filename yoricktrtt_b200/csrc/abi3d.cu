@@ -367,6 +367,55 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   // It must not start before the previous call's read-back of out64 is done.
   TRTT_CK(cudaEventRecord(D.ev[0], st));
   TRTT_CK(cudaStreamWaitEvent(cp, D.ev[0], 0));
+  if (job == 0 && fact) {
+    // Column-factorised views: the only failure (a voxel in the source
+    // plane) is a property of the column geometry, so it is checked first;
+    // the projection then runs in view chunks and each chunk's result is
+    // added into `out` and read back while the next chunk is projected.
+    TRTT_CK(launch_check_columns(P, D.geom.as<View3D>(), (int)nviews, D.err.as<int>(), st));
+    count_launch();
+    int herr = 0;
+    TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRTT_CK(cudaStreamSynchronize(st));
+    if (herr & TRTT_ERR_SOURCE_PLANE) {
+      std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
+      return fail("a voxel lies in the source plane (wk == 0)");
+    }
+    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
+    TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
+    Fwd3DLaunch L;
+    L.P = P;
+    L.vol = D.vol32.as<float>();
+    L.gate_stride = nvox;
+    L.sino_view_stride = nu * nv;
+    int rows = 0, warps = 16;
+    choose_band((int)nu, (int)nv, rows, warps);
+    L.band_rows = rows;
+    L.warps = warps;
+    L.err = D.err.as<int>();
+    const int nchunk = (int)std::min<long>(nviews, 6);
+    const long per = (nviews + nchunk - 1) / nchunk;
+    for (int c = 0; c * per < nviews; ++c) {
+      const long v0 = c * per, v1 = std::min<long>(nviews, v0 + per);
+      const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
+      L.views = D.geom.as<View3D>() + v0;
+      L.nviews = (int)(v1 - v0);
+      L.sino = D.det32.as<float>() + off;
+      TRTT_CK(launch_fwd3d(L, st));
+      TRTT_CK(cudaEventRecord(D.ev[2 + c], st));
+      TRTT_CK(cudaStreamWaitEvent(cp, D.ev[2 + c], 0));
+      TRTT_CK(f32_add_to_f64(D.det32.as<float>() + off, D.out64.as<double>() + off, cnt, cp));
+      TRTT_CK(cudaMemcpyAsync(out + off, D.out64.as<double>() + off, sizeof(double) * cnt,
+                              cudaMemcpyDeviceToHost, cp));
+      count_launch(3);
+    }
+    TRTT_CK(cudaEventRecord(D.ev[1], cp));
+    TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
+    TRTT_CK(cudaStreamSynchronize(st));
+    return 0;
+  }
   if (job == 0) {
     TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
     TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));

@@ -52,6 +52,9 @@ struct Back3DLaunch {
 
 cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st);
 cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st);
+// source-plane test of every column of column-factorised views (err |= flag)
+cudaError_t launch_check_columns(const Params3D &P, const View3D *views, int nviews, int *err,
+                                 cudaStream_t st);
 // closed-form model on factorised views, packed FP32x2 (proj3d_fast.cu)
 cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st);
 cudaError_t launch_back3d_fast(const Back3DLaunch &L, cudaStream_t st);

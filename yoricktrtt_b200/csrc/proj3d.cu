@@ -431,6 +431,42 @@ static cudaError_t launch_back(const Back3DLaunch &L, cudaStream_t st)
   return cudaGetLastError();
 }
 
+// Geometry pre-check of column-factorised views: the source-plane
+// condition of every column of every view, evaluated by the same
+// column_geo() the projectors use, so that a caller can learn before any
+// projection whether the call will fail.
+template <int GEOM, int MODEL>
+__global__ void k_check_columns(const Params3D P, const View3D *__restrict__ views, int nviews,
+                                int *__restrict__ err)
+{
+  const long ncols = (long)P.nx * P.ny;
+  const long total = ncols * nviews;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int v = (int)(t / ncols);
+    const int col = (int)(t - (long)v * ncols);
+    ColGeo<MODEL> c;
+    column_geo<GEOM, MODEL>(P, views[v], col % P.nx, col / P.nx, 0, c);
+    if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+  }
+}
+
+cudaError_t launch_check_columns(const Params3D &P, const View3D *views, int nviews, int *err,
+                                 cudaStream_t st)
+{
+  const long total = (long)P.nx * P.ny * nviews;
+  long b = (total + 255) / 256;
+  if (b > 148L * 16) b = 148L * 16;
+  const unsigned grid = (unsigned)(b > 0 ? b : 1);
+  if (P.geom == GEOM_CONE) {
+    if (P.model == MODEL_TABLE) k_check_columns<GEOM_CONE, MODEL_TABLE><<<grid, 256, 0, st>>>(P, views, nviews, err);
+    else k_check_columns<GEOM_CONE, MODEL_CUBIC><<<grid, 256, 0, st>>>(P, views, nviews, err);
+  } else {
+    if (P.model == MODEL_TABLE) k_check_columns<GEOM_PARALLEL, MODEL_TABLE><<<grid, 256, 0, st>>>(P, views, nviews, err);
+    else k_check_columns<GEOM_PARALLEL, MODEL_CUBIC><<<grid, 256, 0, st>>>(P, views, nviews, err);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st)
 {
   if (L.P.model == MODEL_CUBIC && L.band_rows > 0) return launch_fwd3d_fast(L, st);
