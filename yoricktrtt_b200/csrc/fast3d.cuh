@@ -74,4 +74,15 @@ __device__ __forceinline__ void voxel_u_pair(const Params3D &P, const View3D &V,
   if (!(isfinite(up.start.y) && isfinite(scl.y))) up.n1 = 0;
 }
 
+// Primitive at the first edge of both voxels of a pair.  A cell range that
+// was not clamped at cell 0 starts at floor(uc - hs), at or left of the
+// support start, where the primitive is 0 (to within FP32 rounding of the
+// edge abscissa, below 1e-24); only ranges clamped at the detector's first
+// cell need the evaluation.  Used by the direct and transpose kernels alike.
+__device__ __forceinline__ float2 first_edge_prim2(const UPair &up)
+{
+  if (up.lo0 > 0 && up.lo1 > 0) return f2(0.0f);
+  return cubic_prim2(up.start);
+}
+
 }  // namespace trtt

@@ -111,7 +111,7 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
         const int L = max(up.n0, up.n1);
         if (L <= 0) continue;
         const float2 xr = mul2(make_float2(x0, x1), up.rho);
-        float2 Fp = cubic_prim2(up.start);
+        float2 Fp = first_edge_prim2(up);
         float2 lf = f2(1.0f);
         for (int l = 0; l < L; ++l) {
           const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
@@ -198,7 +198,7 @@ __device__ __forceinline__ void column_profile(const Params3D &P, const View3D &
     const int L = max(up.n0, up.n1);
     if (L <= 0) continue;
     const float2 xr = mul2(make_float2(x0, x1), up.rho);
-    float2 Fp = cubic_prim2(up.start);
+    float2 Fp = first_edge_prim2(up);
     float2 lf = f2(1.0f);
     for (int l = 0; l < L; ++l) {
       const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
@@ -429,7 +429,7 @@ k_fwd3d_pull(const Params3D P, const View3D *__restrict__ views,
         const int L = max(up.n0, up.n1);
         if (L <= 0) continue;
         const float2 xr = mul2(make_float2(x0, x1), up.rho);
-        float2 Fp = cubic_prim2(up.start);
+        float2 Fp = first_edge_prim2(up);
         float2 lf = f2(1.0f);
         for (int l = 0; l < L; ++l) {
           const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
@@ -606,7 +606,7 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
       for (int p = 0; p < KP; ++p) {
         const int L = max(up[p].n0, up[p].n1);
         if (L <= 0) continue;
-        float2 Fp = cubic_prim2(up[p].start);
+        float2 Fp = first_edge_prim2(up[p]);
         float2 S = f2(0.f);
         float2 lf = f2(1.0f);
         for (int l = 0; l < L; ++l) {
