@@ -136,10 +136,12 @@ def cpu_pair_sample(nviews_sample, threads=None):
     views = np.linspace(0, VIEWS - 1, nviews_sample).astype(int)
 
     def work(vs):
+        out = np.zeros((ND, ND))  # private outputs, one pair per thread
+        back = np.zeros_like(vol)
         for v in vs:
-            out = np.zeros((ND, ND))
+            out.fill(0.0)
             orc.cb3d(out, vol, sc, int(v), 0)
-            back = np.zeros_like(vol)
+            back.fill(0.0)
             orc.cb3d(back, det_in, sc, int(v), 1)
 
     chunks = [views[t::threads] for t in range(threads)]
@@ -163,8 +165,10 @@ def run_reference(args):
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle build failed: {e}"}))
         return 0
-    cores = os.cpu_count() or 1
-    sample = max(1, min(cores, 8))
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    # one view pair per host thread (at most 256 threads: each holds a private
+    # FP64 output volume of 134 MB)
+    sample = max(1, min(cores, VIEWS, 256))
     times = []
     for it in range(args.warmup + args.steps):
         val, dt, kind, thr = cpu_pair_sample(sample, cores)
