@@ -782,7 +782,9 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   a.rh = 128 * S + 2 * a.g.wp + 2;
   a.cs = ((a.rh * 16 + 127) / 128) * 128 + 64;
   a.stage_bytes = ((2 * a.cs + 288 * n + 1023) / 1024) * 1024;
-  a.nstg = 4 * a.stage_bytes <= 112 * 1024 ? 4 : 3;
+  // a tile with at most 3 stages (16 input channels) has all of them in
+  // flight from the start: 3 buffers, and one more CTA per SM
+  a.nstg = (3 * a.groups <= 3 || 4 * a.stage_bytes > 112 * 1024) ? 3 : 4;
   int smem = a.nstg * a.stage_bytes;
   a.tmem_cols = pow2_cols(S * n);
   smem = residency_smem(smem, a.tmem_cols);
