@@ -37,6 +37,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "runtime.h"
@@ -276,7 +277,7 @@ struct WgradArgs {
   long r0, r1;          // rows summed over
   int kt;               // rows (K) per stage: 128 or 256
   int steps;            // kt-row stages per CTA
-  int csa, csb, a_bytes, stage_bytes, nstg;
+  int csa, csb, a_bytes, b_bytes, nstg;  // A regions of all stages, then B regions
   uint32_t tmem_cols;
 };
 
@@ -303,8 +304,9 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
   }
   // Only the cout/8 real chunks of the A operand are staged; the M = 64
   // MMAs read the rows above cout from whatever follows them in shared
-  // memory (inside the allocation, which has a tail for the last stage):
-  // those accumulator rows are never read back.
+  // memory (the A regions of all stages come first, then the B regions, and
+  // the allocation has a tail where those do not reach 8 chunk strides past
+  // the last A region): those accumulator rows are never read back.
   if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
   tc::fence_before_sync();
   __syncthreads();
@@ -313,7 +315,8 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
 
   auto load = [&](int it, int buf) {
     const long q0 = qbeg + (long)it * KT;
-    const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
+    const uint32_t as = sbase + (uint32_t)(buf * a.a_bytes);
+    const uint32_t bs = sbase + (uint32_t)(nstg * a.a_bytes + buf * a.b_bytes);
     for (int e = tid; e < KT * nca; e += 128) {
       const int r = e / nca, c = e - nca * (e / nca);
       const long row = q0 + r;
@@ -352,7 +355,8 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
     if (tid == 0) {
       tc::fence_after_sync();
       const int buf = it % nstg;
-      const uint32_t as = sbase + (uint32_t)(buf * a.stage_bytes), bs = as + (uint32_t)a.a_bytes;
+      const uint32_t as = sbase + (uint32_t)(buf * a.a_bytes);
+      const uint32_t bs = sbase + (uint32_t)(nstg * a.a_bytes + buf * a.b_bytes);
       // the three accumulators alternate so that consecutive MMAs are independent
 #pragma unroll 4
       for (int ks = 0; ks < KT / 16; ++ks) {
@@ -708,7 +712,7 @@ int residency_smem(int smem, uint32_t tmem_cols)
 // CTAs still fit on an SM, else 128; row ranges split into chunks so that
 // the grid (9 x chunks) covers the GPU about four times.
 struct WgradPlan {
-  int kt, csa, csb, a_bytes, stage_bytes, nstg, smem;
+  int kt, csa, csb, a_bytes, b_bytes, nstg, smem;
   long chunks, steps;
   uint32_t tmem_cols;
 };
@@ -725,11 +729,14 @@ WgradPlan wgrad_plan(int cout, int cin, const Grid3 &g)
     p.csa = kt * 16 + pad_a;
     p.csb = (((kt + 2) * 16 + 127) / 128) * 128 + pad_b;
     p.a_bytes = ((nca * p.csa + 127) / 128) * 128;
-    p.stage_bytes = ((p.a_bytes + ncb * p.csb + 1023) / 1024) * 1024;
-    p.nstg = 4 * p.stage_bytes <= 112 * 1024 ? 4 : 3;
-    // tail: the last stage's MMAs read 8 chunk strides of A rows
-    const int tail = (((8 - nca) * p.csa + 127) / 128) * 128;
-    p.smem = residency_smem(p.nstg * p.stage_bytes + tail, p.tmem_cols);
+    p.b_bytes = ((ncb * p.csb + 127) / 128) * 128;
+    const int stage = p.a_bytes + p.b_bytes;
+    p.nstg = 4 * stage <= 112 * 1024 ? 4 : 3;
+    // the last stage's MMAs read 8 chunk strides from its A region
+    const int body = p.nstg * stage;
+    const int reach = (p.nstg - 1) * p.a_bytes + 8 * p.csa;
+    const int total = ((std::max(body, reach) + 1023) / 1024) * 1024;
+    p.smem = residency_smem(total, p.tmem_cols);
     if (p.smem <= 112 * 1024) break;
   }
   const long total = (g.rows - 2 * g.plane + p.kt - 1) / p.kt;
@@ -838,7 +845,7 @@ int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, cons
   a.csa = pl.csa;
   a.csb = pl.csb;
   a.a_bytes = pl.a_bytes;
-  a.stage_bytes = pl.stage_bytes;
+  a.b_bytes = pl.b_bytes;
   a.nstg = pl.nstg;
   a.tmem_cols = pl.tmem_cols;
   const int smem = pl.smem;
