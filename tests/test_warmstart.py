@@ -33,8 +33,9 @@ def test_learned_start_against_zero_and_backprojection():
     assert i0.converged and il.converged
     # both runs end at the same optimum (the plain method judges the result);
     # the relative-change stopping rule leaves the final objectives of
-    # different starts scattered by about 1e-4
-    assert abs(il.f[-1] - i0.f[-1]) <= 3e-4 * i0.f[-1]
+    # different starts (and of repeated runs: the summation order of the
+    # atomics varies) scattered by a few 1e-4
+    assert abs(il.f[-1] - i0.f[-1]) <= 1e-3 * i0.f[-1]
     assert float(torch.linalg.norm(xl - x0) / torch.linalg.norm(x0)) <= 0.05
     # the warm-started run starts below the zero start's objective after
     # its first iterations: the first iterate of the plain run that gets as

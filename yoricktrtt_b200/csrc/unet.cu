@@ -710,7 +710,8 @@ int residency_smem(int smem, uint32_t tmem_cols)
 
 // Stage layout of the weight-gradient kernel: 256 rows per stage when two
 // CTAs still fit on an SM, else 128; row ranges split into chunks so that
-// the grid (9 x chunks) covers the GPU about four times.
+// the grid (9 x chunks) fills about four waves of resident CTAs, each CTA
+// running at least 16 stages where the volume is large enough.
 struct WgradPlan {
   int kt, csa, csb, a_bytes, b_bytes, nstg, smem;
   long chunks, steps;
@@ -740,7 +741,13 @@ WgradPlan wgrad_plan(int cout, int cin, const Grid3 &g)
     if (p.smem <= 112 * 1024) break;
   }
   const long total = (g.rows - 2 * g.plane + p.kt - 1) / p.kt;
-  long chunks = 592 / 9;
+  // about four full waves of resident CTAs (shared memory and tensor-memory
+  // columns bound the CTAs per SM) over the 9 (dz, dy) groups
+  int per_sm = kSmemPerSM / (p.smem + 2048);
+  per_sm = std::max(1, std::min(per_sm, 512 / (int)p.tmem_cols));
+  long chunks = std::max(1L, 4L * 148 * per_sm / 9);  // 9 chunks never exceed 4 waves
+  // at least 16 stages per CTA, unless that leaves fewer than 65 chunks
+  chunks = std::min(chunks, std::max(65L, total / 16));
   if (chunks > total) chunks = total;
   if (chunks < 1) chunks = 1;
   p.steps = (total + chunks - 1) / chunks;
