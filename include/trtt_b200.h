@@ -290,7 +290,11 @@ int trtt_b200_spline_sample(const float *x, float *z, float *tmp, long nx, long 
  * NULL) receive maxiter + 1 objective values / wall-clock seconds since the
  * start (entry k after iteration k).  info->converged: 1 stopping rule met,
  * 2 zero projected gradient, 0 iteration limit, -1 line search failed.
- * Work buffers are allocated for the call (about 2 mem + 14 volumes). */
+ * Work buffers (2 mem + 14 volumes and 2 detector stacks) are allocated on
+ * the first call and kept for later calls with the same sizes on the same
+ * device (a reconstruction loop over many data sets then allocates once);
+ * a call with other sizes frees and reallocates them.  Calls are
+ * serialised by a process-wide lock. */
 typedef struct {
   int iterations, evaluations, converged;
   double f_first, f_last, seconds;

@@ -176,7 +176,8 @@ enum {
 };
 
 // Work buffers are kept between calls with the same sizes (a reconstruction
-// loop over many samples then allocates once); released at exit.
+// loop over many samples then allocates once) and freed when the sizes
+// change; the last set is held until the process exits.
 struct Workspace {
   std::mutex mu;
   int device = -1;
