@@ -378,6 +378,15 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
                             int accumulate, const float *resid, int nb, int d, int h, int w,
                             void *stream);
 size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w);
+/* Shared-memory plan the convolution kernels use for a shape (host only, no
+ * GPU needed; for checks of the staging arithmetic).  which = 0: forward /
+ * input-gradient kernel with cin input and cout output channels, info[0..7]
+ * = sub-tiles S, slab rows, chunk stride, stage bytes, stages, dynamic shared
+ * memory, tensor-memory columns, tiles.  which = 1: weight gradient,
+ * info[0..9] = rows per stage, A and B chunk strides, A and B region bytes,
+ * stages, dynamic shared memory, tensor-memory columns, row chunks, stages
+ * per chunk. */
+int trtt_b200_conv3_plan_info(int which, int cin, int cout, int nb, int d, int h, int w, long *info);
 int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2,
                           float *dw, float *db, void *scratch, size_t scratch_bytes, int nb, int d,
                           int h, int w, void *stream);

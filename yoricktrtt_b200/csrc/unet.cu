@@ -708,6 +708,32 @@ int residency_smem(int smem, uint32_t tmem_cols)
   return smem < need ? need : smem;
 }
 
+// Stage layout of the forward / input-gradient kernel (S = 2 sub-tiles of
+// 128 rows per CTA): slab of 128 S + 2 (w+2) + 2 rows per 8-channel chunk,
+// two chunks and the 9 tap tiles of the weights per stage.
+constexpr int kFwdS = 2;
+struct FwdPlan {
+  int rh, cs, stage_bytes, nstg, smem;
+  long tiles;
+  uint32_t tmem_cols;
+};
+
+FwdPlan fwd_plan(int n, int groups, const Grid3 &g)
+{
+  FwdPlan p;
+  p.rh = 128 * kFwdS + 2 * g.wp + 2;
+  p.cs = ((p.rh * 16 + 127) / 128) * 128 + 64;
+  p.stage_bytes = ((2 * p.cs + 288 * n + 1023) / 1024) * 1024;
+  // a tile with at most 3 stages (16 input channels) has all of them in
+  // flight from the start: 3 buffers, and one more CTA per SM
+  p.nstg = (3 * groups <= 3 || 4 * p.stage_bytes > 112 * 1024) ? 3 : 4;
+  p.tmem_cols = pow2_cols(kFwdS * n);
+  p.smem = residency_smem(p.nstg * p.stage_bytes, p.tmem_cols);
+  const long span = g.rows - 2 * g.plane;
+  p.tiles = (span + 128 * kFwdS - 1) / (128 * kFwdS);
+  return p;
+}
+
 // Stage layout of the weight-gradient kernel: 256 rows per stage when two
 // CTAs still fit on an SM, else 128; row ranges split into chunks so that
 // the grid (9 x chunks) fills about four waves of resident CTAs, each CTA
@@ -782,7 +808,7 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   if (mode == kFwdGrad && (n1 < 0 || n1 > n || n1 % 16 || (n1 < n && !y2)))
     return fail("conv3_forward: bad channel split");
   if (!grid_ok(nb, d, h, w)) return fail("conv3_forward: bad grid");
-  constexpr int S = 2;
+  constexpr int S = kFwdS;
   FwdArgs a;
   a.x1 = static_cast<const bf16 *>(x1);
   a.x2 = static_cast<const bf16 *>(x2);
@@ -793,18 +819,15 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   a.resid = resid;
   a.g = make_grid(nb, d, h, w);
   a.row0 = a.g.plane;
-  a.rh = 128 * S + 2 * a.g.wp + 2;
-  a.cs = ((a.rh * 16 + 127) / 128) * 128 + 64;
-  a.stage_bytes = ((2 * a.cs + 288 * n + 1023) / 1024) * 1024;
-  // a tile with at most 3 stages (16 input channels) has all of them in
-  // flight from the start: 3 buffers, and one more CTA per SM
-  a.nstg = (3 * a.groups <= 3 || 4 * a.stage_bytes > 112 * 1024) ? 3 : 4;
-  int smem = a.nstg * a.stage_bytes;
-  a.tmem_cols = pow2_cols(S * n);
-  smem = residency_smem(smem, a.tmem_cols);
+  const FwdPlan pl = fwd_plan(n, a.groups, a.g);
+  a.rh = pl.rh;
+  a.cs = pl.cs;
+  a.stage_bytes = pl.stage_bytes;
+  a.nstg = pl.nstg;
+  a.tmem_cols = pl.tmem_cols;
+  const int smem = pl.smem;
   if (smem > 227 * 1024) return fail("conv3_forward: volume rows too long for the staged slab");
-  const long span = a.g.rows - 2 * a.g.plane;
-  const long tiles = (span + 128 * S - 1) / (128 * S);
+  const long tiles = pl.tiles;
   if (tiles <= 0 || tiles > 0x7FFFFFFFL) return fail("conv3_forward: bad tile count");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TRTT_CK(set_smem(k_conv3_fwd<S>, smem));
@@ -812,6 +835,28 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   count_launch();
   TRTT_CK(cudaGetLastError());
   return 0;
+}
+
+int trtt_b200_conv3_plan_info(int which, int cin, int cout, int nb, int d, int h, int w, long *info)
+{
+  using namespace trtt;
+  clear_error();
+  if (!info || !grid_ok(nb, d, h, w) || cin <= 0 || cout <= 0 || cin % 16 || cout % 16)
+    return fail("conv3_plan_info: bad arguments");
+  const Grid3 g = make_grid(nb, d, h, w);
+  if (which == 0) {
+    const FwdPlan p = fwd_plan(cout, cin / 16, g);
+    const long v[] = {kFwdS, p.rh, p.cs, p.stage_bytes, p.nstg, p.smem, p.tmem_cols, p.tiles};
+    for (int i = 0; i < 8; ++i) info[i] = v[i];
+    return 0;
+  }
+  if (which == 1) {
+    const WgradPlan p = wgrad_plan(cout, cin, g);
+    const long v[] = {p.kt, p.csa, p.csb, p.a_bytes, p.b_bytes, p.nstg, p.smem, p.tmem_cols, p.chunks, p.steps};
+    for (int i = 0; i < 10; ++i) info[i] = v[i];
+    return 0;
+  }
+  return fail("conv3_plan_info: which must be 0 (forward) or 1 (weight gradient)");
 }
 
 size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w)
