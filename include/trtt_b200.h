@@ -192,8 +192,21 @@ int trtt_b200_plan3d_status(trtt_b200_plan3d *plan, void *stream);
  * with that many detector rows per CTA and `warps` warps per CTA (0 keeps
  * the current value).  band_rows == TRTT_B200_TILES_PULL: closed-form model,
  * atomic-free band kernel (each detector cell accumulated in registers by one
- * owning thread; nu <= 512).  Other band_rows < 0: the per-voxel kernel. */
+ * owning thread; nu <= 512).  band_rows == TRTT_B200_TILES_TENSOR: closed-form
+ * model, band accumulated on the tensor cores (tcgen05 kind::tf32, each
+ * value split into two TF32 parts; nu <= 1536, band height chosen from nu).
+ * Its accumulation in tensor memory rounds toward zero: about 1.5e-5 relative
+ * error at 256^3 -> 512^2 where the default kernels stay below 1e-6, so it is
+ * never chosen automatically.  Other band_rows < 0: the per-voxel kernel. */
 #define TRTT_B200_TILES_PULL (-2)
+#define TRTT_B200_TILES_TENSOR (-3)
+
+/* Host-only: the shared-memory plan of the tensor-core band kernel for an
+ * nu-cell-wide detector, info[10] = {band rows, 128-cell u chunks, ring
+ * groups, TMEM columns, A bytes and B bytes of one group, profile floats per
+ * warp, dynamic shared memory, producer warps, columns per group}; -1 if nu
+ * is too wide. */
+int trtt_b200_fwd3d_tc_plan_info(int nu, long *info);
 int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps);
 
 /* Band kernel variant (closed-form model): cols = 1 one column at a time
@@ -257,6 +270,18 @@ int trtt_b200_cb3d_batch(double *out, const double *in, long nx, long ny,
                          long nu, long nv, double u_scl, double v_scl,
                          long nviews, const double *xos, const double *xsd,
                          int geometry, int job);
+
+/* Same call with a choice of accumulation: accumulate != 0 is
+ * trtt_b200_cb3d_batch (out += ...); accumulate == 0 overwrites out with
+ * the projection (out = H in / out = H^T in): the host array is only
+ * written, so it need not be cleared nor copied to the device. */
+int trtt_b200_cb3d_batch_ex(double *out, const double *in, long nx, long ny,
+                            long nz, double s_scl, int s_deg,
+                            const double *cum_footprint, long size_footprint,
+                            double step_footprint, const double *coord_footprint,
+                            long nu, long nv, double u_scl, double v_scl,
+                            long nviews, const double *xos, const double *xsd,
+                            int geometry, int job, int accumulate);
 
 /* Reconstruction helpers (device pointers, FP32 data, FP64 scalars).  The
  * FP64 results are ADDED into *f_dev / *out_dev (device scalars), so several

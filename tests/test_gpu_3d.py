@@ -264,6 +264,44 @@ def test_batch_entry_point_transpose_chunks(oracle_port):
         assert rel_l2(out - 0.5, (call + 1) * ref) <= TOL
 
 
+@pytest.mark.parametrize("tilted", [False, True])
+@pytest.mark.parametrize("job", [0, 1])
+def test_batch_entry_point_overwrite(oracle_port, tilted, job):
+    """trtt_b200_cb3d_batch_ex with accumulate == 0: `out` (filled with NaN
+    here) is replaced by the projection, for column-factorised (circular)
+    and per-voxel (tilted) views; accumulate == 1 equals the plain call."""
+    from yoricktrtt_b200 import _lib
+    sc = _tilted_scan(G.TRTT_CONE_BEAM, views=7) if tilted else _scan(G.TRTT_CONE_BEAM, views=7)
+    rng = np.random.default_rng(11)
+    vol = _vol(sc, seed=3)
+    det = rng.random((sc.nviews, sc.nv, sc.nu))
+    inp = vol if job == 0 else det
+    shape = (sc.nviews, sc.nv, sc.nu) if job == 0 else vol.shape
+    ref = np.zeros(shape)
+    for v in range(sc.nviews):
+        if job == 0:
+            oracle_port.cb3d(ref[v], vol, sc, v, 0)
+        else:
+            oracle_port.cb3d(ref, np.ascontiguousarray(det[v]), sc, v, 1)
+    lib = _lib.load()
+    xos, xsd = np.ascontiguousarray(sc.xos), np.ascontiguousarray(sc.xsd)
+
+    def call(out, acc):
+        rc = lib.trtt_b200_cb3d_batch_ex(
+            _lib.dptr(out), _lib.dptr(inp), sc.nx, sc.ny, sc.nz, sc.s_scl, sc.s_deg, None, 0,
+            1.0, None, sc.nu, sc.nv, sc.u_scl, sc.v_scl, sc.nviews, _lib.dptr(xos),
+            _lib.dptr(xsd), 4, job, acc)
+        assert rc == 0, _lib.last_error()
+
+    out = np.full(shape, np.nan)
+    call(out, 0)
+    assert np.isfinite(out).all() and rel_l2(out, ref) <= TOL
+    call(out, 0)  # again: still replaced, not doubled
+    assert rel_l2(out, ref) <= TOL
+    call(out, 1)
+    assert rel_l2(out, 2 * ref) <= TOL
+
+
 @pytest.mark.parametrize("model", ["cubic", "table"])
 def test_4d_gates(oracle_port, model):
     """Per-gate projection of the 4D path: view k sees
@@ -298,3 +336,66 @@ def test_4d_gates(oracle_port, model):
         else:
             ref_back[g0] += w1 * bt  # repeated index: the second write wins
     assert rel_l2(back, ref_back) <= TOL
+
+
+TC_CASES = [
+    (G.TRTT_CONE_BEAM, {}),                                    # nu 40: one u chunk, band > nv
+    (G.TRTT_PARALLEL_BEAM, {}),
+    (G.TRTT_CONE_BEAM, dict(nu=22, nv=18)),                    # clipped footprints
+    (G.TRTT_CONE_BEAM, dict(us=0.7, vs=1.3, s=0.8)),           # anisotropic
+    (G.TRTT_CONE_BEAM, dict(u_off=3.3, v_off=-2.1)),           # detector offsets
+    (G.TRTT_CONE_BEAM, dict(nu=300, nv=140, us=0.15, vs=0.2)), # 3 u chunks, several bands
+    (G.TRTT_CONE_BEAM, dict(nu=640, nv=70, us=0.08, vs=0.5)),  # 5 chunks, one-group ring
+]
+
+
+@pytest.mark.parametrize("mode,kw", TC_CASES)
+def test_tensor_band_kernel(oracle_port, mode, kw):
+    """Direct projector with the band accumulated on the tensor cores
+    (set_tiles(-3, 0), TF32 split in three products) against the FP64
+    oracle, accumulating onto a non-zero detector; the status flag stays
+    clear."""
+    import torch
+    from yoricktrtt_b200.projectors import Projector3D
+    name = "CB3D" if mode == G.TRTT_CONE_BEAM else "PB3D"
+    sc = _scan(mode, views=6, **kw)
+    vol = _vol(sc, seed=17)
+    pr = Projector3D(sc)
+    assert pr.factorized
+    pr.set_tiles(-3, 0)
+    xt = torch.tensor(vol, dtype=torch.float32, device="cuda")
+    pre = torch.rand(sc.nviews, sc.nv, sc.nu, device="cuda")
+    det = pr.forward(xt, out=pre.clone())
+    pr.status()
+    det = (det - pre).double().cpu().numpy()
+    for v in range(sc.nviews):
+        ref = np.zeros((sc.nv, sc.nu))
+        assert oracle_port._p3d(name, ref, vol, sc, v, 0, None) == 0
+        assert rel_l2(det[v], ref) <= TOL, (v, rel_l2(det[v], ref))
+
+
+def test_tensor_band_kernel_gates_and_empty(oracle_port):
+    """4D per-gate direct projection and an all-zero volume (no column
+    reaches the tensor cores) through the tensor-core band kernel."""
+    import torch
+    from yoricktrtt_b200.projectors import Projector3D
+    nt = 3
+    sc = _scan(G.TRTT_CONE_BEAM, views=5)
+    gates = np.stack([_vol(sc, seed=40 + g) for g in range(nt)])
+    t_index = np.array([0.0, 0.6, 1.5, 2.2, 2.9])
+    pr = Projector3D(sc)
+    pr.set_gates(nt, t_index)
+    pr.set_tiles(-3, 0)
+    det = pr.forward(torch.tensor(gates, dtype=torch.float32, device="cuda")).double().cpu().numpy()
+    for k, t in enumerate(t_index):
+        (g0, g1), (w0, w1) = G.gate_weights(t, nt)
+        ref = np.zeros((sc.nv, sc.nu))
+        oracle_port.cb3d(ref, np.ascontiguousarray(w0 * gates[g0] + w1 * gates[g1]), sc, k, 0)
+        assert rel_l2(det[k], ref) <= TOL
+    pr2 = Projector3D(sc)
+    pr2.set_tiles(-3, 0)
+    zero = torch.zeros(pr2.volume_shape(), device="cuda")
+    out = torch.full((sc.nviews, sc.nv, sc.nu), 0.25, device="cuda")
+    pr2.forward(zero, out=out)
+    pr2.status()
+    assert torch.all(out == 0.25)

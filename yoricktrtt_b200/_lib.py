@@ -72,11 +72,14 @@ SIGNATURES = {
     "trtt_b200_spline_sample": (_I, [_vp, _vp, _vp, _L, _L, _L, _vp]),
     "trtt_b200_cb3d_batch": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
                                    _D, _L, _dp, _dp, _I, _I]),
+    "trtt_b200_cb3d_batch_ex": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _L, _D, _dp, _L, _L, _D,
+                                      _D, _L, _dp, _dp, _I, _I, _I]),
     "trtt_b200_conv3_pack": (_I, [_vp, _I, _I, _I, _vp, _vp]),
     "trtt_b200_conv3_forward": (_I, [_vp, _I, _vp, _I, _vp, _I, _vp, _I, C.c_float, _vp, _vp, _I,
                                       _I, _vp, _I, _I, _I, _I, _vp]),
     "trtt_b200_conv3_wgrad_scratch": (C.c_size_t, [_I, _I, _I, _I, _I, _I]),
     "trtt_b200_conv3_plan_info": (_I, [_I, _I, _I, _I, _I, _I, _I, _lp]),
+    "trtt_b200_fwd3d_tc_plan_info": (_I, [_I, _lp]),
     "trtt_b200_conv3_wgrad": (_I, [_vp, _I, _vp, _I, _vp, _I, _vp, _vp, _vp, C.c_size_t, _I, _I,
                                     _I, _I, _vp]),
     "trtt_b200_unet_resample": (_I, [_vp, _vp, _I, _I, _I, _I, _I, _I, _I, _vp]),

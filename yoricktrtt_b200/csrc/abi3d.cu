@@ -28,6 +28,7 @@ struct trtt_b200_plan3d {
   int nt = 1;
   int band_rows = 0, warps = 16;
   int pull = 0;  // 1: atomic-free band kernel (closed-form model, nu <= 512)
+  int tc = 0;    // 1: tensor-core band kernel (closed-form model)
   int cols = 1;  // 2: column-pair band kernel (closed-form model)
   bool factorized = true;
   DevBuf views, cum, gate_ptr, entries, scratch, err;
@@ -154,14 +155,25 @@ extern "C" int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *pl, int band_rows, i
   if (!pl) return fail("plan3d_set_tiles: null plan");
   if (band_rows == 0 && warps == 0) {  // defaults
     pl->pull = 0;
+    pl->tc = 0;
     choose_band(pl->P.nu, pl->P.nv, pl->band_rows, pl->warps);
     return 0;
   }
   if (band_rows == TRTT_B200_TILES_PULL) {  // atomic-free band kernel
     pl->pull = 1;
+    pl->tc = 0;
+    return 0;
+  }
+  if (band_rows == TRTT_B200_TILES_TENSOR) {  // tensor-core band kernel
+    if (fwd3d_tc_band_rows((int)pl->P.nu, (int)pl->P.nv) <= 0)
+      return fail("plan3d_set_tiles: detector too wide for the tensor-core band kernel");
+    pl->pull = 0;
+    pl->tc = 1;
+    if (pl->band_rows <= 0) choose_band(pl->P.nu, pl->P.nv, pl->band_rows, pl->warps);
     return 0;
   }
   pl->pull = 0;
+  pl->tc = 0;
   if (warps > 0) {
     if (warps < 2 || warps > 16) return fail("plan3d_set_tiles: warps must be in [2, 16]");
     pl->warps = warps;
@@ -246,6 +258,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
     L.band_rows = pl->factorized ? pl->band_rows : 0;
     L.warps = pl->warps;
     L.pull = pl->pull;
+    L.tc = pl->tc;
     L.cols = pl->cols;
     L.err = pl->err.as<int>();
     TRTT_CK(launch_fwd3d(L, st));
@@ -320,10 +333,45 @@ namespace {
 
 // One call of a 3D projector on host double* arrays for `nviews` views:
 // out += H in (job 0) or out += H^T in (job != 0), reference layouts.
+// View chunks of the host-buffer pipeline, as boundaries (chunks + 1
+// entries).  Only one copy per call cannot overlap a kernel: the read-back
+// of the direct projection's last chunk and the upload of the transpose's
+// first chunk.  The direct projection therefore runs full chunks and ends
+// with a chunk of one wave of CTAs (`tail` views); the transpose starts with
+// `head` views and grows its chunks by half each time (each upload hides
+// behind the previous chunk's kernel) up to `full` views.  At most `cap`
+// chunks (the event pool).
+std::vector<long> fwd_chunks(long nviews, long full, long tail, int cap)
+{
+  std::vector<long> b{0};
+  tail = std::max<long>(1, std::min(tail, nviews));
+  const long mid = nviews - tail;
+  if (mid > 0) {
+    const long n = std::min<long>(std::max<long>(1, (mid + full - 1) / full), cap - 1);
+    for (long c = 0; c < n; ++c) b.push_back(b.back() + mid / n + (c < mid % n ? 1 : 0));
+  }
+  b.push_back(nviews);
+  return b;
+}
+
+std::vector<long> back_chunks(long nviews, long head, long full, int cap)
+{
+  std::vector<long> b{0};
+  double size = (double)std::max<long>(1, head);
+  while (b.back() < nviews) {
+    long c = std::min<long>((long)size, nviews - b.back());
+    if ((int)b.size() == cap) c = nviews - b.back();
+    b.push_back(b.back() + c);
+    size = std::min<double>(size * 1.5, (double)std::max<long>(1, full));
+  }
+  return b;
+}
+
 int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
            double s_scl, int s_deg, const double *cum, long size, double step,
            const double *coord, long nu, long nv, double u_scl, double v_scl,
-           long nviews, const double *xos, const double *xsd, int job)
+           long nviews, const double *xos, const double *xsd, int job,
+           bool accumulate = true)
 {
   clear_error();
   if (!out || !in || !xos || !xsd) return fail("null array argument");
@@ -363,15 +411,22 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   TRTT_CK(D.det32.ensure(sizeof(float) * npix));
   cudaStream_t cp = D.copy;
   // The copy stream brings `out` to the device while the kernels run (it is
-  // only read there: the host array is written after the error check).
-  // It must not start before the previous call's read-back of out64 is done.
+  // only read there: the host array is written after the error check); with
+  // accumulate == false the device copy starts from zeros instead and `out`
+  // is only written.  Either must not start before the previous call's
+  // read-back of out64 is done.
   TRTT_CK(cudaEventRecord(D.ev[0], st));
   TRTT_CK(cudaStreamWaitEvent(cp, D.ev[0], 0));
+  auto out_to_device = [&](cudaStream_t s) -> cudaError_t {
+    if (accumulate) return cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);
+    return cudaMemsetAsync(D.out64.p, 0, sizeof(double) * nout, s);
+  };
   if (job == 0 && fact) {
     // Column-factorised views: the only failure (a voxel in the source
     // plane) is a property of the column geometry, so it is checked first;
-    // the projection then runs in view chunks and each chunk's result is
-    // added into `out` and read back while the next chunk is projected.
+    // the projection then runs in view chunks (fwd_chunks) and each chunk's
+    // result is added into `out` and read back while the next chunk is
+    // projected.
     TRTT_CK(launch_check_columns(P, D.geom.as<View3D>(), (int)nviews, D.err.as<int>(), st));
     count_launch();
     int herr = 0;
@@ -382,7 +437,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
       return fail("a voxel lies in the source plane (wk == 0)");
     }
     TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
-    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(out_to_device(cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
     Fwd3DLaunch L;
@@ -395,10 +450,11 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     L.band_rows = rows;
     L.warps = warps;
     L.err = D.err.as<int>();
-    const int nchunk = (int)std::min<long>(nviews, 6);
-    const long per = (nviews + nchunk - 1) / nchunk;
-    for (int c = 0; c * per < nviews; ++c) {
-      const long v0 = c * per, v1 = std::min<long>(nviews, v0 + per);
+    const long bands = (nv + rows - 1) / rows;
+    const std::vector<long> cb = fwd_chunks(nviews, (nviews + 5) / 6, std::max<long>(1, 2L * D.sms / bands),
+                                            DropIn::kEvents - 2);
+    for (size_t c = 0; c + 1 < cb.size(); ++c) {
+      const long v0 = cb[c], v1 = cb[c + 1];
       const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
       L.views = D.geom.as<View3D>() + v0;
       L.nviews = (int)(v1 - v0);
@@ -418,7 +474,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   }
   if (job == 0) {
     TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
-    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
@@ -458,13 +514,13 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     L.gate_stride = nvox;
     L.factorized = fact ? 1 : 0;
     L.err = D.err.as<int>();
-    // the detector stack arrives in (at most 6) view chunks on the copy
+    // the detector stack arrives in view chunks (back_chunks) on the copy
     // stream; each chunk is projected back (accumulating into the volume)
     // as soon as it is on the device, while the next chunk is copied
-    const int nchunk = (int)std::min<long>(nviews, 6);
-    const int per = (int)((nviews + nchunk - 1) / nchunk);
-    for (int c = 0; c * per < nviews; ++c) {
-      const long v0 = (long)c * per, v1 = std::min<long>(nviews, v0 + per);
+    const std::vector<long> cb = back_chunks(nviews, std::max<long>(1, nviews / 32), (nviews + 5) / 6,
+                                             DropIn::kEvents - 2);
+    for (size_t c = 0; c + 1 < cb.size(); ++c) {
+      const long v0 = cb[c], v1 = cb[c + 1];
       const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
       TRTT_CK(cudaMemcpyAsync(D.in64.as<double>() + off, in + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, cp));
       TRTT_CK(f64_to_f32(D.in64.as<double>() + off, D.det32.as<float>() + off, cnt, cp));
@@ -476,7 +532,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
       TRTT_CK(launch_back3d(L, st));
       count_launch(2);
     }
-    TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
   }
   TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
@@ -558,6 +614,21 @@ int trtt_b200_cb3d_batch(double *out, const double *in, long nx, long ny, long n
   return host3d(g, out, in, nx, ny, nz, s_scl, s_deg, cum_footprint, size_footprint,
                 step_footprint, coord_footprint, nu, nv, u_scl, v_scl, nviews, xos, xsd,
                 job);
+}
+
+int trtt_b200_cb3d_batch_ex(double *out, const double *in, long nx, long ny, long nz,
+                            double s_scl, int s_deg, const double *cum_footprint,
+                            long size_footprint, double step_footprint,
+                            const double *coord_footprint, long nu, long nv,
+                            double u_scl, double v_scl, long nviews,
+                            const double *xos, const double *xsd, int geometry,
+                            int job, int accumulate)
+{
+  const int g = geom_code(geometry);
+  if (g < 0) return fail("cb3d_batch_ex: geometry must be 3, 4 or 5");
+  return host3d(g, out, in, nx, ny, nz, s_scl, s_deg, cum_footprint, size_footprint,
+                step_footprint, coord_footprint, nu, nv, u_scl, v_scl, nviews, xos, xsd,
+                job, accumulate != 0);
 }
 
 }  // extern "C"

@@ -5,6 +5,8 @@
 // voxel_u_pair() and cubic_prim2(), so the pair stays an exact adjoint.
 #pragma once
 
+#include <climits>
+
 #include "geom3d.cuh"
 
 namespace trtt {
@@ -83,6 +85,79 @@ __device__ __forceinline__ float2 first_edge_prim2(const UPair &up)
 {
   if (up.lo0 > 0 && up.lo1 > 0) return f2(0.0f);
   return cubic_prim2(up.start);
+}
+
+// Column helpers shared by the direct kernels ----------------------------
+
+static constexpr unsigned FULLM = 0xffffffffu;
+
+__device__ __forceinline__ ColGeo<MODEL_CUBIC> shfl_colc(const ColGeo<MODEL_CUBIC> &c, int src)
+{
+  ColGeo<MODEL_CUBIC> r;
+  r.vax.lo = __shfl_sync(FULLM, c.vax.lo, src);
+  r.vax.n = __shfl_sync(FULLM, c.vax.n, src);
+  r.vax.start = __shfl_sync(FULLM, c.vax.start, src);
+  r.vax.inc = __shfl_sync(FULLM, c.vax.inc, src);
+  r.bad = 0;
+  r.A = __shfl_sync(FULLM, c.A, src);
+  r.B = __shfl_sync(FULLM, c.B, src);
+  r.h_u0m = __shfl_sync(FULLM, c.h_u0m, src);
+  r.rho0c = __shfl_sync(FULLM, c.rho0c, src);
+  r.inv_den = __shfl_sync(FULLM, c.inv_den, src);
+  return r;
+}
+
+__device__ __forceinline__ float vox_val(const float *__restrict__ vol, long gate_stride,
+                                         const View3D &V, long idx)
+{
+  float x = __ldg(vol + (long)V.g0 * gate_stride + idx);
+  if (V.w1 != 0.0f) return fmaf(V.w0, x, V.w1 * __ldg(vol + (long)V.g1 * gate_stride + idx));
+  return V.w0 == 1.0f ? x : V.w0 * x;
+}
+
+// Profile of one column: prof[u] += sum_k rho_k x_k (F(e_{u+1,k}) - F(e_{u,k}))
+// (shared-memory atomics), returns the warp-uniform cell range [lo, hi).
+template <int GEOM>
+__device__ __forceinline__ void column_profile(const Params3D &P, const View3D &V, const float *__restrict__ vol,
+                                               long gate_stride, const ColGeo<MODEL_CUBIC> &cc, int col,
+                                               float *prof, int lane, int &lo_out, int &hi_out)
+{
+  const int nz = P.nz;
+  int lo = INT_MAX, hi = INT_MIN;
+  const long cbase = (long)col * nz;
+  for (int k0 = lane; k0 < nz; k0 += 64) {
+    const int k1 = k0 + 32;
+    const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
+    const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+    if (x0 == 0.0f && x1 == 0.0f) continue;
+    UPair up;
+    voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+    if (x0 == 0.0f) up.n0 = 0;
+    if (x1 == 0.0f) up.n1 = 0;
+    const int L = max(up.n0, up.n1);
+    if (L <= 0) continue;
+    const float2 xr = mul2(make_float2(x0, x1), up.rho);
+    float2 Fp = first_edge_prim2(up);
+    float2 lf = f2(1.0f);
+    for (int l = 0; l < L; ++l) {
+      const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+      const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
+      if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
+      if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
+      Fp = F;
+      lf = add2(lf, f2(1.0f));
+    }
+    if (up.n0 > 0) {
+      lo = min(lo, up.lo0);
+      hi = max(hi, up.lo0 + up.n0);
+    }
+    if (up.n1 > 0) {
+      lo = min(lo, up.lo1);
+      hi = max(hi, up.lo1 + up.n1);
+    }
+  }
+  lo_out = __reduce_min_sync(FULLM, lo);
+  hi_out = __reduce_max_sync(FULLM, hi);
 }
 
 }  // namespace trtt

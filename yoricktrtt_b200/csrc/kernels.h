@@ -12,6 +12,7 @@ namespace trtt {
 enum : int {
   TRTT_ERR_SOURCE_PLANE = 1,  // a voxel lies in the source plane (wk == 0)
   TRTT_ERR_BAD_INDEX = 2,     // sparse index out of range
+  TRTT_ERR_STALL = 4,         // a bounded wait gave up (tensor-core band kernel)
 };
 
 // One (view, weight) contribution to a gate in the transpose.
@@ -32,6 +33,7 @@ struct Fwd3DLaunch {
   int warps;             // warps per CTA of the band kernel
   int pull = 0;          // closed-form model, nu <= 512: atomic-free band kernel
   int cols = 1;          // closed-form model: 2 = column-pair band kernel
+  int tc = 0;            // closed-form model: 1 = tensor-core band kernel (rows chosen by it)
   int *err;              // device error flags
 };
 
@@ -72,5 +74,11 @@ cudaError_t col_f32_add_to_xyz_f32(const float *src, float *dst, int nx,
                                    int ny, int nz, int nb, cudaStream_t st);
 cudaError_t f64_to_f32(const double *src, float *dst, long n, cudaStream_t st);
 cudaError_t f32_add_to_f64(const float *src, double *dst, long n, cudaStream_t st);
+
+// Tensor-core band kernel of the direct projector (closed-form model,
+// column-factorised views): its detector-row band height for an nu x nv
+// detector, 0 if the detector is too wide for it (nu > 2048).
+int fwd3d_tc_band_rows(int nu, int nv);
+cudaError_t launch_fwd3d_tc(const Fwd3DLaunch &L, cudaStream_t st);
 
 }  // namespace trtt

@@ -68,6 +68,8 @@ cudaError_t DropIn::init()
   }
   e = cudaSetDevice(device);
   if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
   e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;
   e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking);

@@ -38,6 +38,7 @@ struct DropIn {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;  // host<->device copies that overlap the kernels
+  int sms = 148;                 // streaming multiprocessors of `device`
   static constexpr int kEvents = 33;
   cudaEvent_t ev[kEvents] = {};
   DevBuf in64, out64, vol32, det32, geom, gates, aux, err;
