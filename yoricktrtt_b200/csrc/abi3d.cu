@@ -452,21 +452,30 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     L.err = D.err.as<int>();
     const long bands = (nv + rows - 1) / rows;
     const std::vector<long> cb = fwd_chunks(nviews, (nviews + 5) / 6, std::max<long>(1, 2L * D.sms / bands),
-                                            DropIn::kEvents - 2);
+                                            DropIn::kChunks);
+    // chunks alternate between two kernel streams (they write disjoint
+    // views), so that the last, partly filled wave of CTAs of one chunk
+    // overlaps the start of the next
+    cudaStream_t ks2 = D.stream2;
+    TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvents - 2], st));
+    TRTT_CK(cudaStreamWaitEvent(ks2, D.ev[DropIn::kEvents - 2], 0));
     for (size_t c = 0; c + 1 < cb.size(); ++c) {
       const long v0 = cb[c], v1 = cb[c + 1];
       const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
+      cudaStream_t ks = (c & 1) ? ks2 : st;
       L.views = D.geom.as<View3D>() + v0;
       L.nviews = (int)(v1 - v0);
       L.sino = D.det32.as<float>() + off;
-      TRTT_CK(launch_fwd3d(L, st));
-      TRTT_CK(cudaEventRecord(D.ev[2 + c], st));
+      TRTT_CK(launch_fwd3d(L, ks));
+      TRTT_CK(cudaEventRecord(D.ev[2 + c], ks));
       TRTT_CK(cudaStreamWaitEvent(cp, D.ev[2 + c], 0));
       TRTT_CK(f32_add_to_f64(D.det32.as<float>() + off, D.out64.as<double>() + off, cnt, cp));
       TRTT_CK(cudaMemcpyAsync(out + off, D.out64.as<double>() + off, sizeof(double) * cnt,
                               cudaMemcpyDeviceToHost, cp));
       count_launch(3);
     }
+    TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvents - 1], ks2));
+    TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvents - 1], 0));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
     TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
     TRTT_CK(cudaStreamSynchronize(st));
@@ -518,7 +527,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     // stream; each chunk is projected back (accumulating into the volume)
     // as soon as it is on the device, while the next chunk is copied
     const std::vector<long> cb = back_chunks(nviews, std::max<long>(1, nviews / 32), (nviews + 5) / 6,
-                                             DropIn::kEvents - 2);
+                                             DropIn::kChunks);
     for (size_t c = 0; c + 1 < cb.size(); ++c) {
       const long v0 = cb[c], v1 = cb[c + 1];
       const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;

@@ -74,6 +74,8 @@ cudaError_t DropIn::init()
   if (e != cudaSuccess) return e;
   e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;
+  e = cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
   for (int i = 0; i < kEvents; ++i) {
     e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
     if (e != cudaSuccess) return e;

@@ -38,8 +38,12 @@ struct DropIn {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;  // host<->device copies that overlap the kernels
+  cudaStream_t stream2 = nullptr;  // second kernel stream: view chunks of the direct projection
   int sms = 148;                 // streaming multiprocessors of `device`
-  static constexpr int kEvents = 33;
+  // ev[0], ev[1]: copy stream start / end; ev[2 + c]: view chunk c (at most
+  // kChunks); ev[kEvents - 2], ev[kEvents - 1]: second kernel stream start / end
+  static constexpr int kChunks = 31;
+  static constexpr int kEvents = kChunks + 4;
   cudaEvent_t ev[kEvents] = {};
   DevBuf in64, out64, vol32, det32, geom, gates, aux, err;
   cudaError_t init();
