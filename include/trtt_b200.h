@@ -258,6 +258,20 @@ int trtt_b200_plan2d_assemble(trtt_b200_plan2d *plan, int max_cells, double *a,
 
 int trtt_b200_plan2d_destroy(trtt_b200_plan2d *plan);
 
+/* Distance-driven 2D projector pair (the reference's Yorick evaluators
+ * _trtt_single_distance_driven_{PB,FB}2D_projector, Ytrtt_2D_projectors.i:
+ * 943-1245) on host FP64 arrays for `nviews` views, accumulating into out:
+ * job 0: out(detector [view][nv]) += H in(image [ny][nx]); job 1:
+ * out(image) += H^T in(detector).  xos / xsd are nviews*12 coefficients of
+ * each view's (xos . xotilt) and xsd transforms, in millimetres (the
+ * distance-driven evaluator does not fold in the pixel and cell transforms,
+ * :868-880).  geometry: TRTT_B200_PARALLEL_BEAM, or TRTT_B200_FAN_BEAM /
+ * TRTT_B200_CONE_BEAM (fan).  Returns -1 (out unchanged) if a fan-beam point
+ * lies in the source plane, as the reference raises an error there. */
+int trtt_b200_dd2d(double *out, const double *in, long nx, long ny, double s_scl, long nv,
+                   double v_scl, long nviews, const double *xos, const double *xsd,
+                   int geometry, int job);
+
 /* Batched host-buffer entry point: the whole scan in one call.  Same
  * conventions as trtt_CB3D/trtt_CB3D_cubic (host double*, accumulate,
  * reference layouts) for `nviews` views: xos/xsd are nviews*12, the

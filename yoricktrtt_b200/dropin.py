@@ -56,6 +56,52 @@ def scan3d_call(name, out, vol, scan, view, job, table=None):
         job, table)
 
 
+def dd2d(out, x, scan, job, view0: int = 0, nview: int | None = None, coefs=None):
+    """Distance-driven 2D projector (``D_single_2D`` / ``D_whole_2D``,
+    Ytrtt_2D_projectors.i:820-1245) for views [view0, view0 + nview) of a
+    ``geometry.Scan2D``: job 0 adds H x (x image [ny][nx]) into out
+    [nview][nv]; job 1 adds H^T x (x [nview][nv]) into out [ny][nx].
+    ``coefs``: (xos, xsd) from ``geometry.dd_coefs_2d`` (computed if None)."""
+    from .geometry import dd_coefs_2d
+    nview = scan.nviews - view0 if nview is None else nview
+    xos, xsd = dd_coefs_2d(scan) if coefs is None else coefs
+    xos = np.ascontiguousarray(xos[view0:view0 + nview], dtype=np.float64)
+    xsd = np.ascontiguousarray(xsd[view0:view0 + nview], dtype=np.float64)
+    shape_in = (scan.ny, scan.nx) if job == 0 else (nview, scan.nv)
+    shape_out = (nview, scan.nv) if job == 0 else (scan.ny, scan.nx)
+    for a, shp, name in ((x, shape_in, "x"), (out, shape_out, "out")):
+        if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != int(np.prod(shp)):
+            raise ValueError(f"{name} must be C-contiguous float64 of shape {shp}")
+    rc = _lib.load().trtt_b200_dd2d(dptr(out), dptr(x), scan.nx, scan.ny, scan.s_scl, scan.nv,
+                                    scan.v_scl, nview, dptr(xos), dptr(xsd), scan.mode, job)
+    _lib.check(rc, "trtt_b200_dd2d")
+
+
+class DistanceDriven2D:
+    """The whole-scan distance-driven operator ``C(x, job)`` of a 2D scan
+    (``D_whole_2D``): job 0 returns the sinogram [nviews][nv] of an image,
+    job 1 the image of a sinogram; ``single_view(k)`` is ``D_single_2D``."""
+
+    def __init__(self, scan):
+        from .geometry import dd_coefs_2d
+        self.scan = scan
+        self.coefs = dd_coefs_2d(scan)
+
+    def __call__(self, x, job: int = 0, view0: int = 0, nview: int | None = None):
+        s = self.scan
+        nview = s.nviews - view0 if nview is None else nview
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros((nview, s.nv) if job == 0 else (s.ny, s.nx))
+        dd2d(out, x, s, job, view0, nview, self.coefs)
+        return out
+
+    def single_view(self, k: int):
+        def op(x, job=0):
+            r = self(np.asarray(x).reshape(-1, self.scan.nv) if job == 1 else x, job, k, 1)
+            return r[0] if job == 0 else r
+        return op
+
+
 def dd_pb3d(out, vol, scan, view, job):
     lib = _lib.load()
     rc = lib.trtt_DD_PB3D(dptr(out), dptr(vol), scan.nx, scan.ny, scan.nz, scan.s_scl,

@@ -280,6 +280,21 @@ def circular_scan_2d(nx, ny, s_scl, s_deg, nv, v_scl, nviews,
                   rsc, rsd)
 
 
+def dd_coefs_2d(scan: "Scan2D"):
+    """Per-view (xos . xotilt).a and xsd.a of a 2D circular scan: the
+    coefficients of the distance-driven projector, which works in object and
+    detector millimetres (Ytrtt_2D_projectors.i:868-880) where the
+    spline-driven ones also carry the pixel and detector-cell transforms."""
+    par = scan.mode == TRTT_PARALLEL_BEAM
+    xos = np.empty((scan.nviews, 12))
+    xsd = np.empty((scan.nviews, 12))
+    for k, th in enumerate(scan.theta):
+        a, b, c = view_xforms(th, None if par else scan.rsc, None if par else scan.rsd)
+        xos[k] = a.combine(c).a
+        xsd[k] = b.a
+    return xos, xsd
+
+
 def gate_weights(t_index: float, nt: int):
     """Linear temporal interpolation of one view between two gates
     (Ytrtt_3D_projectors.i:301-311): j = [floor(t), ceil(t)] mod nt and
