@@ -256,6 +256,19 @@ int trtt_b200_plan2d_status(trtt_b200_plan2d *plan, void *stream);
 int trtt_b200_plan2d_assemble(trtt_b200_plan2d *plan, int max_cells, double *a,
                               long *rows, long *cols, void *stream);
 
+/* y (+)= A x for a sparse matrix in compressed rows (device arrays, FP64,
+ * 0-based column indices): the sparse-product mode of the 2D projectors
+ * (the matrix of trtt_b200_plan2d_assemble once sorted into rows, for H or
+ * for H^T), which the reference evaluates with trtt_mvmult
+ * (plugin/trtt_common.c:62-69; Tomography_2D/Ytrtt2D_optim.i:320-387).
+ * row_ptr has nrows + 1 entries; accumulate == 0 overwrites y.  Entries with
+ * a column index outside [0, ncols) are skipped and flagged; asynchronous on
+ * `stream`.  csr_status synchronises `stream` and returns -1 (clearing the
+ * flag) if a product since the last call skipped an entry. */
+int trtt_b200_csr_spmv(const long *row_ptr, const long *col, const double *val, long nrows,
+                       long ncols, const double *x, double *y, int accumulate, void *stream);
+int trtt_b200_csr_status(void *stream);
+
 int trtt_b200_plan2d_destroy(trtt_b200_plan2d *plan);
 
 /* Distance-driven 2D projector pair (the reference's Yorick evaluators

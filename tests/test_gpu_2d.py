@@ -101,6 +101,54 @@ def test_assembly_matches_sparser(oracle_port):
     lib.trtt_b200_plan2d_destroy(h)
 
 
+@pytest.mark.parametrize("mode,name", [(G.TRTT_PARALLEL_BEAM, "PB2D"), (G.TRTT_FAN_BEAM, "FB2D")])
+@pytest.mark.parametrize("model", ["cubic", "table"])
+def test_sparse_system_products(oracle_port, mode, name, model):
+    """Precomputed-matrix mode: H assembled on the GPU, sorted into
+    compressed rows, H x and H^T y by trtt_b200_csr_spmv in FP64 against the
+    FP64 oracle projector; accumulate adds onto the output."""
+    import torch
+    from yoricktrtt_b200.recon import Projector2D
+    sc = _scan2d(mode, nx=20, ny=16, nv=40, views=5)
+    table = TABLE if model == "table" else None
+    S = Projector2D(sc, table).sparse_system(max_cells=32)
+    rng = np.random.default_rng(9)
+    img = _img(sc, seed=4)
+    y = rng.random((sc.nviews, sc.nv))
+    f = S.forward(torch.tensor(img, dtype=torch.float64, device="cuda"))
+    b = S.backward(torch.tensor(y, dtype=torch.float64, device="cuda"))
+    S.status()
+    f, b = f.cpu().numpy(), b.cpu().numpy()
+    ref_b = np.zeros((sc.ny, sc.nx))
+    for v in range(sc.nviews):
+        ref = np.zeros(sc.nv)
+        assert oracle_port.p2d(name, ref, img, sc, v, 0, table) == 0
+        assert np.abs(f[v] - ref).max() <= 1e-12 * np.abs(ref).max()
+        oracle_port.p2d(name, ref_b, np.ascontiguousarray(y[v]), sc, v, 1, table)
+    assert np.abs(b - ref_b).max() <= 1e-12 * np.abs(ref_b).max()
+    pre = torch.full((sc.nviews, sc.nv), 0.25, dtype=torch.float64, device="cuda")
+    S.forward(torch.tensor(img, dtype=torch.float64, device="cuda"), out=pre, accumulate=True)
+    assert np.abs(pre.cpu().numpy() - 0.25 - f).max() <= 1e-14 * np.abs(f).max()
+
+
+def test_sparse_product_bad_index_flag():
+    """A column index outside the matrix is skipped and reported by
+    trtt_b200_csr_status (no out-of-range read)."""
+    import torch
+    from yoricktrtt_b200.recon import _ptr, _stream
+    lib = _lib.load()
+    rp = torch.tensor([0, 2, 3], dtype=torch.int64, device="cuda")
+    col = torch.tensor([0, 5, 1], dtype=torch.int64, device="cuda")   # 5 >= ncols = 2
+    val = torch.tensor([1.0, 7.0, 2.0], dtype=torch.float64, device="cuda")
+    x = torch.tensor([3.0, 4.0], dtype=torch.float64, device="cuda")
+    y = torch.zeros(2, dtype=torch.float64, device="cuda")
+    _lib.check(lib.trtt_b200_csr_spmv(_ptr(rp), _ptr(col), _ptr(val), 2, 2, _ptr(x), _ptr(y), 0,
+                                      _stream()), "csr_spmv")
+    assert lib.trtt_b200_csr_status(_stream()) == -1
+    assert y.tolist() == [3.0, 8.0]
+    assert lib.trtt_b200_csr_status(_stream()) == 0
+
+
 def _lf_params(nx=40, ny=36, nd=120, vs=2.0, ps=1.0, sd=300.0, dd=150.0, off=(0.0, 0.0)):
     from oracle.oracle import LF2DParams as OP
     kw = dict(pixelSize=ps, pixelStep=ps, voxelSize=vs, sourceDistance=sd,

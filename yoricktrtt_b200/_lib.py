@@ -81,6 +81,8 @@ SIGNATURES = {
     "trtt_b200_conv3_plan_info": (_I, [_I, _I, _I, _I, _I, _I, _I, _lp]),
     "trtt_b200_fwd3d_tc_plan_info": (_I, [_I, _lp]),
     "trtt_b200_dd2d": (_I, [_dp, _dp, _L, _L, _D, _L, _D, _L, _dp, _dp, _I, _I]),
+    "trtt_b200_csr_spmv": (_I, [_vp, _vp, _vp, _L, _L, _vp, _vp, _I, _vp]),
+    "trtt_b200_csr_status": (_I, [_vp]),
     "trtt_b200_conv3_wgrad": (_I, [_vp, _I, _vp, _I, _vp, _I, _vp, _vp, _vp, C.c_size_t, _I, _I,
                                     _I, _I, _vp]),
     "trtt_b200_unet_resample": (_I, [_vp, _vp, _I, _I, _I, _I, _I, _I, _I, _vp]),

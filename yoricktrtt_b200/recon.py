@@ -25,6 +25,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import time
+import warnings
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -127,6 +128,11 @@ class Projector2D:
     def status(self):
         _lib.check(_lib.load().trtt_b200_plan2d_status(self._h, _stream()), "projector")
 
+    def sparse_system(self, max_cells: int = 64) -> "SparseSystem2D":
+        """The plan's system matrix H, assembled once, for sparse products
+        (B-spline plans only)."""
+        return SparseSystem2D(self, max_cells)
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().trtt_b200_plan2d_destroy(self._h)
@@ -137,6 +143,66 @@ class Projector2D:
             self.close()
         except Exception:
             pass
+
+
+class SparseSystem2D:
+    """Precomputed-matrix mode of a 2D B-spline plan (the reference's sparse
+    system, Ytrtt_2D_projectors.i:212-369, applied with trtt_mvmult in
+    Tomography_2D/Ytrtt2D_optim.i:320-387).  H (nviews*nv x ny*nx) is
+    assembled on the GPU by trtt_b200_plan2d_assemble, sorted once into
+    compressed rows for H and for H^T (torch's sparse conversion, done
+    once), and every product is one trtt_b200_csr_spmv launch in FP64.
+    Images are (ny, nx), sinograms (nviews, nv), float64 CUDA tensors."""
+
+    def __init__(self, plan: Projector2D, max_cells: int = 64):
+        torch = _torch()
+        lib = _lib.load()
+        self.nx, self.ny, self.nv, self.nviews = plan.nx, plan.ny, plan.nv, plan.nviews
+        npix = self.nx * self.ny
+        n = self.nviews * npix * max_cells
+        a = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = torch.zeros(n, dtype=torch.int64, device="cuda")
+        c = torch.zeros(n, dtype=torch.int64, device="cuda")
+        _lib.check(lib.trtt_b200_plan2d_assemble(plan._h, max_cells, _ptr(a), _ptr(r), _ptr(c),
+                                                 _stream()), "trtt_b200_plan2d_assemble")
+        plan.status()  # a footprint wider than max_cells or a source-plane pixel raises here
+        view = torch.arange(n, device="cuda") // (npix * max_cells)
+        keep = r > 0
+        rows = view[keep] * self.nv + (r[keep] - 1)
+        cols = c[keep] - 1
+        vals = a[keep]
+        shape = (self.nviews * self.nv, npix)
+        with warnings.catch_warnings():  # torch flags its CSR layout as beta; only the sort is used
+            warnings.simplefilter("ignore", UserWarning)
+            h = torch.sparse_coo_tensor(torch.stack([rows, cols]), vals, shape).coalesce().to_sparse_csr()
+            ht = torch.sparse_coo_tensor(torch.stack([cols, rows]), vals,
+                                         shape[::-1]).coalesce().to_sparse_csr()
+        self._h = (h.crow_indices().contiguous(), h.col_indices().contiguous(), h.values().contiguous())
+        self._ht = (ht.crow_indices().contiguous(), ht.col_indices().contiguous(), ht.values().contiguous())
+        self.nnz = int(vals.numel())
+
+    def _apply(self, m, nrows, ncols, x, out, accumulate):
+        _lib.check(_lib.load().trtt_b200_csr_spmv(_ptr(m[0]), _ptr(m[1]), _ptr(m[2]), nrows, ncols,
+                                                  _ptr(x), _ptr(out), 1 if accumulate else 0,
+                                                  _stream()), "trtt_b200_csr_spmv")
+        return out
+
+    def forward(self, x, out=None, accumulate=False):
+        """H x: image (ny, nx) -> sinogram (nviews, nv)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.nviews, self.nv, dtype=torch.float64, device=x.device)
+        return self._apply(self._h, self.nviews * self.nv, self.nx * self.ny, x.contiguous(), out, accumulate)
+
+    def backward(self, y, out=None, accumulate=False):
+        """H^T y: sinogram (nviews, nv) -> image (ny, nx)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.ny, self.nx, dtype=torch.float64, device=y.device)
+        return self._apply(self._ht, self.nx * self.ny, self.nviews * self.nv, y.contiguous(), out, accumulate)
+
+    def status(self):
+        _lib.check(_lib.load().trtt_b200_csr_status(_stream()), "sparse product")
 
 
 class Objective:
