@@ -14,7 +14,8 @@
   parallel and fan beam 2D and parallel and cone beam 3D: relative L2 error
   of a few 1e-3 (2D) and 1e-2 (3D), shrinking with the voxel size, while the
   same comparison with a mirrored or axis-swapped phantom is off by >10%,
-  which pins the orientation of the detector axes.
+  which pins the orientation of the detector axes; the same for the
+  reference's distance-driven parallel-beam projector (trtt_DD_PB3D).
 """
 import math
 import os
@@ -228,6 +229,26 @@ def test_3d_projectors_match_analytic(oracle_port, mode, name):
     swapped = np.ascontiguousarray(np.swapaxes(vol, 1, 2))
     o = np.zeros((sc.nv, sc.nu))
     oracle_port._p3d(name, o, swapped, sc, 1, 0, None)
+    assert rel_l2(o, ana[1]) > 0.1
+
+
+def test_dd_pb3d_matches_analytic(oracle_port):
+    """The reference's distance-driven parallel-beam projector (trtt_DD_PB3D,
+    compiled restatement) converges to the analytic ellipsoid projections and
+    conserves each view's mass; swapping x and y is far off."""
+    errs = []
+    for n, s in ((64, 1.5), (96, 1.0)):
+        sc = G.circular_scan_3d(n, n, n, s, 3, 100, 100, 1.6, 1.6, 4, mode=G.TRTT_PARALLEL_BEAM)
+        vol = A.ellipsoid_volume(ELLIPSOIDS[:2], n, n, n, s, 2)
+        ana = A.projections_3d(ELLIPSOIDS[:2], sc)
+        out = np.zeros((sc.nviews, sc.nv, sc.nu))
+        for k in range(sc.nviews):
+            assert oracle_port.dd_pb3d(out[k], vol, sc, k, 0) == 0
+        errs.append(rel_l2(out, ana))
+        assert out.sum(axis=(1, 2)) == pytest.approx(np.full(sc.nviews, vol.sum() * s ** 3), rel=1e-9)
+    assert errs[1] <= 0.012 and errs[1] < errs[0]
+    o = np.zeros((sc.nv, sc.nu))
+    oracle_port.dd_pb3d(o, np.ascontiguousarray(np.swapaxes(vol, 1, 2)), sc, 1, 0)
     assert rel_l2(o, ana[1]) > 0.1
 
 
