@@ -14,8 +14,18 @@
 // one cell, [max(p_i, v_d), min(p_i+1, v_d+1)], which is what these kernels
 // compute directly, with the reference's order of the products.
 //
-//   k_dd2d_fwd : one thread per (view, cell); for every slice a binary search
-//                over the monotone boundaries finds the pixels under the cell.
+//   k_dd2d_fwd : one CTA per view and block of DD_THREADS * DD_CPT cells; for
+//                every slice the CTA tabulates the slice's projected
+//                boundaries (and, in fan beam, the pixels' distortion *
+//                magnification) in shared memory once, and each thread finds
+//                the pixels under its cells by binary search in the table.
+//   k_dd2d_fwd_cell: one thread per (view, cell), boundaries evaluated where
+//                needed (the same arithmetic).  Fan beam uses the table (each
+//                boundary costs two divisions; 512^2, 720 views, 1024 cells:
+//                8.9 ms against 21.9 ms); parallel beam, whose boundaries are
+//                one multiply-add, and images too wide for the table use this
+//                kernel, which runs more threads (512^2, 360 views: 3.1 ms
+//                against 4.1 ms).
 //   k_dd2d_back: one thread per pixel, summing over views (no atomics).
 //
 // In parallel beam the boundaries are equally spaced, so mean|dp| is the
@@ -24,6 +34,7 @@
 // sets TRTT_ERR_SOURCE_PLANE.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -75,8 +86,76 @@ __device__ __forceinline__ double cell_edge(const DD2DParams &P, int d)
   return ((double)d - 0.5 * P.nv) * P.v_scl;
 }
 
-__global__ void k_dd2d_fwd(DD2DParams P, const DDView2D *__restrict__ views, const double *__restrict__ img,
-                           double *__restrict__ sino, int *__restrict__ err)
+constexpr int DD_THREADS = 256;  // threads of the tabulating direct kernel
+constexpr int DD_CPT = 4;        // detector cells per thread
+
+__global__ void __launch_bounds__(DD_THREADS)
+k_dd2d_fwd(DD2DParams P, const DDView2D *__restrict__ views, const double *__restrict__ img,
+           double *__restrict__ sino, int *__restrict__ err)
+{
+  extern __shared__ double tab[];
+  const int v = blockIdx.x;
+  const DDView2D V = views[v];
+  const int na = V.y_active ? P.ny : P.nx, npas = V.y_active ? P.nx : P.ny;
+  double *pb = tab;           // na + 1 projected boundaries of the current slice
+  double *hm = tab + na + 1;  // fan beam: distortion * magnification * s^2 of its na pixels
+  const int base = blockIdx.y * (DD_THREADS * DD_CPT) + threadIdx.x;
+  double acc[DD_CPT];
+#pragma unroll
+  for (int c = 0; c < DD_CPT; ++c) acc[c] = 0.0;
+  for (int q = 0; q < npas; ++q) {
+    const double cq = ((double)q - 0.5 * (npas - 1)) * P.s;  // passive centre
+    __syncthreads();
+    for (int k = threadIdx.x; k <= na; k += DD_THREADS) {
+      const double c = ((double)k - 0.5 * na) * P.s;
+      pb[k] = V.y_active ? dd_proj(V, P.fan, cq, c, err) : dd_proj(V, P.fan, c, cq, err);
+    }
+    if (P.fan) {
+      for (int i = threadIdx.x; i < na; i += DD_THREADS) {
+        const double ci = ((double)i - 0.5 * (na - 1)) * P.s;
+        hm[i] = (V.y_active ? dd_dm(V, cq, ci) : dd_dm(V, ci, cq)) * (P.s * P.s);
+      }
+    }
+    __syncthreads();
+    const double p0 = pb[0], pn = pb[na];
+    const bool inc = pn >= p0;
+    const double smin = inc ? p0 : pn, smax = inc ? pn : p0;
+#pragma unroll
+    for (int c = 0; c < DD_CPT; ++c) {
+      const int d = base + c * DD_THREADS;
+      if (d >= P.nv) break;
+      const double vlo = cell_edge(P, d), vhi = cell_edge(P, d + 1);
+      if (smax <= vlo || smin >= vhi) continue;
+      int a = 0, b = na + 1;  // first k with P'(k) > vlo, P'(k) = pb[inc ? k : na - k]
+      while (a < b) {
+        const int m = (a + b) >> 1;
+        if (pb[inc ? m : na - m] > vlo) b = m;
+        else a = m + 1;
+      }
+      int k = a > 0 ? a - 1 : 0;
+      double pk = pb[inc ? k : na - k];
+      for (; k < na && pk < vhi; ++k) {
+        const double pk1 = pb[inc ? k + 1 : na - k - 1];
+        const double ov = fmin(pk1, vhi) - fmax(pk, vlo);
+        if (ov > 0.0) {
+          const int i = inc ? k : na - 1 - k;
+          const double x = V.y_active ? img[(long)i * P.nx + q] : img[(long)q * P.nx + i];
+          if (P.fan) acc[c] += ov * ((hm[i] * (1.0 / (pk1 - pk))) * x);
+          else acc[c] += (V.h * ov) * x;
+        }
+        pk = pk1;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < DD_CPT; ++c) {
+    const int d = base + c * DD_THREADS;
+    if (d < P.nv) sino[(long)v * P.nv + d] += acc[c];
+  }
+}
+
+__global__ void k_dd2d_fwd_cell(DD2DParams P, const DDView2D *__restrict__ views, const double *__restrict__ img,
+                                double *__restrict__ sino, int *__restrict__ err)
 {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
@@ -223,8 +302,19 @@ extern "C" int trtt_b200_dd2d(double *out, const double *in, long nx, long ny, d
   TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, st));
   const DDView2D *dv = reinterpret_cast<const DDView2D *>(D.geom.p);
   if (job == 0) {
-    dim3 grid((unsigned)((nv + 127) / 128), (unsigned)nviews);
-    k_dd2d_fwd<<<grid, 128, 0, st>>>(P, dv, D.in64.as<double>(), D.out64.as<double>(), D.err.as<int>());
+    // table of the tabulating kernel: the boundaries and pixel weights of the
+    // longer axis, which is the active one in some views
+    const size_t tab = sizeof(double) * (2 * (size_t)std::max(nx, ny) + 1);
+    if (fan && tab <= 200 * 1024) {
+      if (tab > 48 * 1024)
+        TRTT_CK(cudaFuncSetAttribute(k_dd2d_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab));
+      dim3 grid((unsigned)nviews, (unsigned)((nv + DD_THREADS * DD_CPT - 1) / (DD_THREADS * DD_CPT)));
+      k_dd2d_fwd<<<grid, DD_THREADS, tab, st>>>(P, dv, D.in64.as<double>(), D.out64.as<double>(),
+                                                D.err.as<int>());
+    } else {
+      dim3 grid((unsigned)((nv + 127) / 128), (unsigned)nviews);
+      k_dd2d_fwd_cell<<<grid, 128, 0, st>>>(P, dv, D.in64.as<double>(), D.out64.as<double>(), D.err.as<int>());
+    }
   } else {
     k_dd2d_back<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(P, dv, D.in64.as<double>(), D.out64.as<double>(),
                                                                 D.err.as<int>());
