@@ -1,6 +1,6 @@
 """Learned warm start: what the trained network (weights shipped in
 yoricktrtt_b200/weights/) gains over the plain method's own starts on a
-held-out seed, with the plain method as the judge of the result."""
+held-out seed, with the plain method as the arbiter of the result."""
 import os
 
 import numpy as np
@@ -31,7 +31,7 @@ def test_learned_start_against_zero_and_backprojection():
     xl, il = pb.reconstruct(y, w, x0=start, frtol=1e-6, maxiter=500)
     pb.pr.status()
     assert i0.converged and il.converged
-    # both runs end at the same optimum (the plain method judges the result);
+    # both runs end at the same optimum (the plain method decides the result);
     # the relative-change stopping rule leaves the final objectives of
     # different starts (and of repeated runs: the summation order of the
     # atomics varies) scattered by a few 1e-4

@@ -6,7 +6,7 @@ The reference starts every VMLM-B reconstruction from zero
 normalised backprojection of the data to an estimate of the converged TV
 reconstruction; VMLM-B then starts from that estimate and runs the
 unchanged iteration to the same stopping rule, so the plain method stays
-the judge of the result (a bad estimate only costs iterations).
+the arbiter of the result (a bad estimate only costs iterations).
 
 Architecture (``UNet3D.LAYERS``): two convolutions per level at 16, 32 and
 64 channels, leaky ReLU, 2x2x2 average pooling down, nearest-neighbour

@@ -10,7 +10,7 @@ Pipeline (all on the GPU):
    ``H'(w y) / H'(w H 1)``, the network input.
 3. ``Problem.reconstruct``: VMLM-B + TV (``recon.vmlmb_native``, the cost
    of ``recon.Objective``), the plain method; run from zero it produces the
-   training targets, and it is the judge of every warm start.
+   training targets, and it is the arbiter of every warm start.
 4. ``train``: the U-Net of ``unet.py`` fitted to (backprojection, converged
    reconstruction) pairs by Adam on the tensor-core kernels.
 5. ``evaluate``: held-out seeds reconstructed from a zero start, from the
