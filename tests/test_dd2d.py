@@ -3,10 +3,13 @@
 Ytrtt_2D_projectors.i:943-1245).
 
 CPU: the FP64 restatement of the reference's merged-boundary algorithm
-(oracle/dd2d_oracle.py, parity unpinned: Yorick cannot run here) agrees with
-an independent overlap formulation, is an adjoint pair, conserves mass in
-parallel beam and converges to analytic line integrals of ellipses (with
-the right orientation: a mirrored phantom is far off).
+(oracle/dd2d_oracle.py; Yorick cannot run here) agrees with an independent
+overlap formulation, is an adjoint pair, conserves mass in parallel beam and
+converges to analytic line integrals of ellipses (with the right
+orientation: a mirrored phantom is far off).  In parallel beam it is pinned
+to compiled reference code: the reference's C distance-driven 3D projector
+(trtt_DD_PB3D) on a one-slice scan gives the same projection up to the
+row height.
 GPU: trtt_b200_dd2d (FP64 kernels) against the oracle at <= 1e-12 relative
 max error, accumulating onto a non-zero output; the operator class; the
 source-plane failure.
@@ -57,6 +60,27 @@ def test_oracle_forms_agree_and_adjoint(mode, shape):
     assert _relmax(b, _oracle(D.dd2d_overlap, sc, det, 1)) <= 1e-13
     lhs, rhs = (f * det).sum(), (img * b).sum()
     assert abs(lhs - rhs) <= 1e-13 * abs(lhs)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_parallel_pinned_to_reference_dd_pb3d(oracle_ref, shape):
+    """Parallel beam pinned to compiled reference code: on a one-slice scan
+    (nz = 1, a 3-row detector whose rows are one voxel high) the centre row
+    of the reference's trtt_DD_PB3D, which averages over the row height s,
+    equals the 2D distance-driven projection divided by s, cell by cell."""
+    nx, ny, nv, s, v = shape
+    th = np.linspace(0.0, np.pi, 7, endpoint=False) + 0.1
+    s2 = G.circular_scan_2d(nx, ny, s, 3, nv, v, len(th), mode=G.TRTT_PARALLEL_BEAM, theta=th)
+    s3 = G.circular_scan_3d(nx, ny, 1, s, 3, 3, nv, s, v, len(th), mode=G.TRTT_PARALLEL_BEAM, theta=th)
+    xo, xs = G.dd_coefs_2d(s2)
+    img = np.random.default_rng(nx * ny).random((ny, nx))
+    for k in range(len(th)):
+        a = np.zeros(nv)
+        D.dd2d(a, img, nx, ny, s, nv, v, xo[k], xs[k], D.PARALLEL, 0)
+        b = np.zeros((nv, 3))
+        assert oracle_ref.dd_pb3d(b, np.ascontiguousarray(img[None]), s3, k, 0) == 0
+        assert _relmax(b[:, 1] * s, a) <= 1e-13
+        assert not b[:, 0].any() and not b[:, 2].any()
 
 
 def test_parallel_mass():
