@@ -19,8 +19,9 @@ Pinning: Yorick is not available here, so the restatement cannot be run
 against the Yorick code itself.  In parallel beam it is pinned to the
 reference's compiled C: the distance-driven 3D projector trtt_DD_PB3D
 (plugin/trtt_3D_projectors.c:1077-1173) on a one-slice scan with a detector
-row one voxel high gives this projection divided by the voxel size, cell by
-cell, to ~1e-14.  Fan beam is unpinned (the reference's cone-beam DD,
+row one voxel high gives this projection times the voxel size, cell by
+cell, to ~1e-14 (except the detector's last cell, which that C projector
+leaves empty).  Fan beam is unpinned (the reference's cone-beam DD,
 plugin/trtt_3D_projectors.c:1340-1434, is commented out); it is
 cross-checked against an independent overlap formulation (``dd2d_overlap``)
 and, at model level, against analytic line integrals of ellipses.
