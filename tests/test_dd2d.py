@@ -9,7 +9,7 @@ converges to analytic line integrals of ellipses (with the right
 orientation: a mirrored phantom is far off).  In parallel beam it is pinned
 to compiled reference code: the reference's C distance-driven 3D projector
 (trtt_DD_PB3D) on a one-slice scan gives the same projection times the
-slice thickness.
+slice thickness; the fan beam converges to it as the source recedes.
 GPU: trtt_b200_dd2d (FP64 kernels) against the oracle at <= 1e-12 relative
 max error, accumulating onto a non-zero output; the operator class; the
 source-plane failure.
@@ -83,6 +83,25 @@ def test_parallel_pinned_to_reference_dd_pb3d(oracle_ref, shape):
         assert oracle_ref.dd_pb3d(b, np.ascontiguousarray(img[None]), s3, k, 0) == 0
         assert np.abs(b[:-1, 1] - s * a[:-1]).max() <= 1e-13 * np.abs(s * a).max()
         assert b[-1, 1] == 0.0 and not b[:, 0].any() and not b[:, 2].any()
+
+
+def test_fan_tends_to_pinned_parallel():
+    """Fan beam tied to the pinned parallel beam: with the detector through
+    the isocentre (rsd = rsc) and the source receding, the fan projection
+    (magnification and distortion -> 1) converges to the parallel one, the
+    difference falling as 1/rsc."""
+    nx, ny, nv = 24, 20, 40
+    th = np.linspace(0.0, 2.0 * np.pi, 9, endpoint=False) + 0.2
+    img = np.random.default_rng(0).random((ny, nx))
+    par = G.circular_scan_2d(nx, ny, 1.0, 3, nv, 1.0, len(th), mode=G.TRTT_PARALLEL_BEAM, theta=th)
+    ref = _oracle(D.dd2d, par, img, 0)
+    errs = []
+    for rsc in (1e3, 1e4, 1e5):
+        fan = G.circular_scan_2d(nx, ny, 1.0, 3, nv, 1.0, len(th), mode=G.TRTT_FAN_BEAM, rsc=rsc,
+                                 rsd=rsc, theta=th)
+        errs.append(_relmax(_oracle(D.dd2d, fan, img, 0), ref))
+    assert errs[2] <= 1e-3
+    assert 5.0 < errs[0] / errs[1] < 20.0 and 5.0 < errs[1] / errs[2] < 20.0
 
 
 def test_parallel_mass():
