@@ -119,6 +119,20 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference plugin (or the oracle port) on host threads
 # ---------------------------------------------------------------------------
+_CPU_INPUTS = []
+
+
+def _cpu_inputs():
+    """Scan, FP64 phantom and one detector image of the workload (built once)."""
+    if not _CPU_INPUTS:
+        from yoricktrtt_b200 import phantoms as P
+        _CPU_INPUTS.extend([scan(0, VIEWS),
+                            np.ascontiguousarray(P.ellipsoids_3d(N, N, N, n=20, seed=0,
+                                                                 dtype=np.float64)),
+                            np.ascontiguousarray(np.random.default_rng(0).random((ND, ND)))])
+    return _CPU_INPUTS
+
+
 def cpu_pair_sample(nviews_sample, threads=None):
     """Time nviews_sample forward+transpose view pairs of the workload with the
     reference C on `threads` host threads (views spread over threads, private
@@ -127,10 +141,7 @@ def cpu_pair_sample(nviews_sample, threads=None):
     from oracle import oracle
     kind = "reference" if oracle.ref_available() else "port"
     orc = oracle.get("ref" if kind == "reference" else "port")
-    from yoricktrtt_b200 import phantoms as P
-    sc = scan(0, VIEWS)
-    vol = np.ascontiguousarray(P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float64))
-    det_in = np.ascontiguousarray(np.random.default_rng(0).random((ND, ND)))
+    sc, vol, det_in = _cpu_inputs()
     threads = threads or (os.cpu_count() or 1)
     threads = max(1, min(threads, nviews_sample))
     views = np.linspace(0, VIEWS - 1, nviews_sample).astype(int)
@@ -155,6 +166,32 @@ def cpu_pair_sample(nviews_sample, threads=None):
     return 2 * nviews_sample / dt, dt, kind, threads
 
 
+def _host_cores():
+    if hasattr(os, "sched_getaffinity"):
+        return len(os.sched_getaffinity(0))
+    return os.cpu_count() or 1
+
+
+def cpu_baseline_measure(warmup=1, steps=2):
+    """The CPU baseline as both arms report it: one forward + transpose view
+    pair per host thread and step (at most 256 threads: each holds a private
+    FP64 output volume of 134 MB), `warmup` untimed steps, the median of
+    `steps` timed ones."""
+    cores = _host_cores()
+    sample = max(1, min(cores, VIEWS, 256))
+    times = []
+    kind = thr = None
+    for it in range(warmup + steps):
+        _, dt, kind, thr = cpu_pair_sample(sample, cores)
+        if it >= warmup:
+            times.append(dt)
+    dt = statistics.median(times)
+    return {"value": 2 * sample / dt, "unit": "projections/s", "cores": thr, "kind": kind,
+            "sample": f"{sample} view pairs (forward + transpose) of the workload per step, one per "
+                      f"host thread, reference C in FP64; {warmup} warm-up + median of {steps} steps",
+            "pairs_per_step": sample, "seconds_per_step": dt}
+
+
 def run_reference(args):
     rank = _env_int("RANK", 0)
     if rank != 0:
@@ -165,26 +202,15 @@ def run_reference(args):
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle build failed: {e}"}))
         return 0
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    # one view pair per host thread (at most 256 threads: each holds a private
-    # FP64 output volume of 134 MB)
-    sample = max(1, min(cores, VIEWS, 256))
-    times = []
-    for it in range(args.warmup + args.steps):
-        val, dt, kind, thr = cpu_pair_sample(sample, cores)
-        if it >= args.warmup:
-            times.append(dt)
-    dt = statistics.median(times)
-    value = 2 * sample / dt
+    cpu = cpu_baseline_measure(warmup=args.warmup, steps=args.steps)
+    value, sample, dt = cpu["value"], cpu["pairs_per_step"], cpu["seconds_per_step"]
     line = {
         "impl": "reference", "metric": "fwd+back projections/s", "value": value,
         "unit": "projections/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": f"{sample} of {VIEWS} view pairs per step"},
-        "cpu_baseline": {"value": value, "unit": "projections/s", "cores": thr, "kind": kind,
-                         "sample": f"{sample} view pairs (forward + transpose) of the workload, "
-                                   f"views spread over {thr} threads"},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -195,29 +221,27 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
-def run_b200(args):
-    import torch
-    import torch.distributed as dist
-    from yoricktrtt_b200 import _lib, phantoms as P
-    from yoricktrtt_b200.projectors import Projector3D, columns_from_xyz
+# names of the kernels the step launches (per direction), for the roofline
+FWD_KERNEL = "k_fwd3d_band_fast (direct, detector-row bands)"
+BACK_KERNEL = "k_back3d_col_fast (transpose, column gather)"
+PARITY_VIEWS = (0, 137, 271)
 
-    world = _env_int("WORLD_SIZE", 1)
-    rank = _env_int("RANK", 0)
-    local = _env_int("LOCAL_RANK", 0)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-    sc = scan(rank)
-    pr = Projector3D(sc)
-    if args.band_rows or args.warps:
-        pr.set_tiles(args.band_rows, args.warps)
-    vol_h = P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float32)
-    x = columns_from_xyz(torch.tensor(vol_h, device=dev))
-    sino = torch.zeros(VIEWS, ND, ND, device=dev)
-    back = torch.zeros_like(x)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+
+def _counters():
+    """ncu counters of the two kernels at this workload, committed under
+    profiles/ (DRAM traffic and executed warp instructions per launch)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "counters_cone256.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def timed_pairs(pr, x, sino, back, flush, steps, warmup, world, barrier):
+    """`warmup` untimed then `steps` timed forward + transpose pairs; returns
+    (total ms, per-step forward ms, per-step transpose ms, launches)."""
+    import torch
+    from yoricktrtt_b200 import _lib
     stream = torch.cuda.current_stream()
 
     def step(ev=None):
@@ -233,48 +257,173 @@ def run_b200(args):
             ev[2].record(stream)
         flush.fill_(1.0)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     pr.status()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = _lib.launch_count()
+    barrier()
+    t_start.record(stream)
+    for k in range(steps):
+        step(evs[k])
+    t_end.record(stream)
+    barrier()
+    launches = _lib.launch_count() - launches0
+    pr.status()
+    return (t_start.elapsed_time(t_end), [e[0].elapsed_time(e[1]) for e in evs],
+            [e[1].elapsed_time(e[2]) for e in evs], launches)
+
+
+def parity_block(pr, sc, vol_h, sino):
+    """Relative L2 of the timed forward output on sampled views against the
+    FP64 reference C, and of the transpose of those views of the timed output
+    (one full 360-view transpose launch, the other views zero) against the
+    reference's sum over them.  Runs outside the timed region."""
+    import concurrent.futures as cf
+    import torch
+    from oracle import oracle
+    kind = "ref" if oracle.ref_available() else "port"
+    orc = oracle.get(kind)
+    vol64 = np.ascontiguousarray(vol_h, dtype=np.float64)
+    views = list(PARITY_VIEWS)
+    got = {v: sino[v].double().cpu().numpy() for v in views}
+    y = torch.zeros_like(sino)
+    for v in views:
+        y[v] = sino[v]
+    b = pr.backward(y, layout="xyz").double().cpu().numpy()
+    pr.status()
+
+    def fwd(v):
+        out = np.zeros((ND, ND))
+        orc.cb3d(out, vol64, sc, v, 0)
+        return out
+
+    def bwd(v):
+        out = np.zeros((N, N, N))
+        orc.cb3d(out, np.ascontiguousarray(got[v]), sc, v, 1)
+        return out
+
+    with cf.ThreadPoolExecutor(max(1, min(2 * len(views), _host_cores()))) as ex:
+        fr = list(ex.map(fwd, views))
+        br = list(ex.map(bwd, views))
+    ferr = [float(np.linalg.norm(got[v] - r) / np.linalg.norm(r)) for v, r in zip(views, fr)]
+    ref_b = sum(br)
+    berr = float(np.linalg.norm(b - ref_b) / np.linalg.norm(ref_b))
+    return {"views": views, "forward_rel_l2": ferr, "transpose_rel_l2": berr,
+            "max_rel_l2": max(ferr + [berr]), "bar": 1e-5,
+            "oracle": ("reference C compiled from its sources, FP64" if kind == "ref"
+                       else "FP64 C restatement (bit-identical to the reference C)")}
+
+
+def run_dropin_e2e(sc, vol_h, nsample=8):
+    """The per-view plugin path a Yorick closure takes: one trtt_CB3D_cubic
+    call per view and direction on host FP64 arrays (pageable, as Yorick's
+    are), accumulating into `out`; `nsample` view pairs, scaled."""
+    from yoricktrtt_b200 import dropin
+    vol64 = np.ascontiguousarray(vol_h, dtype=np.float64)
+    out = np.zeros((ND, ND))
+    back = np.zeros((N, N, N))
+    views = np.linspace(0, VIEWS - 1, nsample + 1).astype(int)
+
+    def pair(v):
+        out.fill(0.0)
+        dropin.scan3d_call("CB3D", out, vol64, sc, int(v), 0)
+        dropin.scan3d_call("CB3D", back, out, sc, int(v), 1)
+
+    pair(views[0])  # warm-up
+    t0 = time.perf_counter()
+    for v in views[1:]:
+        pair(v)
+    dt = (time.perf_counter() - t0) / nsample
+    nvox, npix = N ** 3, ND * ND
+    return {"value": 2 / dt, "unit": "projections/s", "ms_per_view_pair": dt * 1e3,
+            "path": "trtt_CB3D_cubic per view and direction (the symbol the Yorick closure "
+                    "_trtt_single_3D_projector calls), pageable host FP64 arrays, out += H in",
+            "sample": f"{nsample} view pairs of the workload, per-pair time scaled to the rate",
+            "h2d_bytes_per_view_pair": 8 * (nvox + npix) + 8 * (npix + nvox),
+            "d2h_bytes_per_view_pair": 8 * npix + 8 * nvox}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from yoricktrtt_b200 import phantoms as P
+    from yoricktrtt_b200.projectors import Projector3D, columns_from_xyz
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    sc = scan(rank)
+    pr = Projector3D(sc)
+    if args.band_rows or args.warps:
+        pr.set_tiles(args.band_rows, args.warps)
+    vol_h = P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float32)
+    x = columns_from_xyz(torch.tensor(vol_h, device=dev))
+    sino = torch.zeros(VIEWS, ND, ND, device=dev)
+    back = torch.zeros_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = _lib.launch_count()
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            v = float(t.item())
+        return v
+
     with ClockSampler(local) as clk:
-        barrier()
-        t_start.record(stream)
-        for k in range(args.steps):
-            step(evs[k])
-        t_end.record(stream)
-        barrier()
-    launches = _lib.launch_count() - launches0
-    ms = t_start.elapsed_time(t_end)
-    fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    back_ms = [e[1].elapsed_time(e[2]) for e in evs]
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    pr.status()
+        ms, fwd_ms, back_ms, launches = timed_pairs(pr, x, sino, back, flush, args.steps,
+                                                    args.warmup, world, barrier)
+    ms = max_over_ranks(ms)
     total_proj = 2 * VIEWS * world * args.steps
     value = total_proj / (ms / 1e3)
+    fwd_avg, back_avg = statistics.mean(fwd_ms), statistics.mean(back_ms)
+    clocks = clk.summary()
+
+    # parity of the timed output (rank 0, outside the timed region)
+    parity = None
+    if rank == 0 and not args.skip_parity:
+        parity = parity_block(pr, sc, vol_h, sino)
+    barrier()
+
+    # the same pair on a dense volume (every voxel non-zero, as a
+    # reconstruction iterate is): no zero-voxel shortcut applies
+    dense = None
+    if not args.skip_dense:
+        rng = np.random.default_rng(1)
+        vd = (vol_h + 0.05 + 0.1 * rng.random(vol_h.shape)).astype(np.float32)
+        xd = columns_from_xyz(torch.tensor(vd, device=dev))
+        dsteps = max(1, min(args.steps, 3))
+        dms, dfwd, dback, _ = timed_pairs(pr, xd, sino, back, flush, dsteps, 1, world, barrier)
+        dms = max_over_ranks(dms)
+        dense = {"value": 2 * VIEWS * world * dsteps / (dms / 1e3), "unit": "projections/s",
+                 "ms_per_step": dms / dsteps, "fwd_ms": statistics.mean(dfwd),
+                 "back_ms": statistics.mean(dback), "steps": dsteps,
+                 "volume": "the phantom + 0.05 + U[0, 0.1): every voxel non-zero"}
+        del xd
 
     # roofline of the dominant kernel: algorithmic bytes per launch (per-view
     # streaming model: the forward reads the volume and writes one detector
     # image per view, the transpose reads one image and writes the volume
-    # contribution per view) / measured launch duration
+    # contribution per view) / measured launch duration; the kernels are
+    # bound by instruction issue, reported beside it from the committed ncu
+    # instruction counts of the same kernels at this workload
     nvox, npix = N ** 3, ND * ND
-    fwd_avg, back_avg = statistics.mean(fwd_ms), statistics.mean(back_ms)
     if back_avg >= fwd_avg:
-        kern, kms = "k_back3d_col_fast (transpose, column gather)", back_avg
+        kern, kms = BACK_KERNEL, back_avg
     else:
-        kern, kms = "k_fwd3d_band_fast (direct, detector-row bands)", fwd_avg
+        kern, kms = FWD_KERNEL, fwd_avg
     alg_bytes = VIEWS * (4 * nvox + 4 * npix)
     peaks = {}
     try:
@@ -284,36 +433,39 @@ def run_b200(args):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (kms / 1e3) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
-            tr = json.load(f)
-        traffic = tr.get(kern.split()[0])
-    except Exception:
-        pass
+    counters = _counters()
+    kc = counters.get("kernels", {}).get(kern.split()[0], {})
+    traffic = kc.get("dram_bytes")
+    issue = None
+    if kc.get("warp_inst"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks.get("sm_mhz") or 1965.0
+        slots = kms * 1e-3 * sms * 4 * mhz * 1e6  # one warp instruction per SMSP and cycle
+        issue = {"warp_inst_per_launch": kc["warp_inst"],
+                 "thread_inst_per_voxel_view": 32.0 * kc["warp_inst"] / (nvox * VIEWS),
+                 "issue_frac": kc["warp_inst"] / slots,
+                 "issue_active_pct_ncu": kc.get("issue_active_pct"),
+                 "peak": f"{sms} SMs x 4 schedulers x 1 warp instruction per cycle at {mhz:g} MHz",
+                 "source": "profiles/counters_cone256.json (" + counters.get("command", "ncu") + ")"}
 
     # end to end through the batched host-buffer C ABI on every rank at once
     # (each rank its own scan), whole-job rate over the slowest rank
     e2e = None
     if not args.skip_e2e:
-        if world > 1:
-            dist.barrier()
+        barrier()
         e2e = run_e2e(sc, vol_h, args, dev)
-        if world > 1:
-            t = torch.tensor([e2e["ms_per_step"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e["ms_per_step"] = float(t.item())
+        e2e["ms_per_step"] = max_over_ranks(e2e["ms_per_step"])
         e2e["value"] = 2 * VIEWS * world / (e2e["ms_per_step"] / 1e3)
         e2e["h2d_bytes_per_step"] *= world  # all ranks
         e2e["d2h_bytes_per_step"] *= world
+    dropin_e2e = None
+    if rank == 0 and world == 1 and not args.skip_e2e:
+        dropin_e2e = run_dropin_e2e(sc, vol_h)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         try:
-            val, dt, kind, thr = cpu_pair_sample(max(1, min(os.cpu_count() or 1, 8)))
-            cpu = {"value": val, "unit": "projections/s", "cores": thr, "kind": kind,
-                   "sample": f"{min(os.cpu_count() or 1, 8)} view pairs (forward + transpose) of the "
-                             f"workload, reference C in FP64, one view per thread ({dt:.1f} s)"}
+            cpu = cpu_baseline_measure(warmup=1, steps=2)
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "unit": "projections/s", "cores": 0, "kind": "port",
                    "sample": f"failed: {e}"}
@@ -330,14 +482,20 @@ def run_b200(args):
                              "the 360-view detector stack (377 MB) exceeds L2",
                        "fwd_ms": fwd_avg, "back_ms": back_avg,
                        "band_rows": args.band_rows or "auto"},
-            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak,
+            "parity": parity,
+            "dense": dense,
+            "roofline": {"bound": "issue", "kernel": kern, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                         "algorithmic_bytes_per_launch": alg_bytes, "issue": issue,
+                         "note": "achieved/peak/frac: the HBM streaming model (not the binding "
+                                 "limit); issue: executed warp instructions per launch over the "
+                                 "launch's issue slots (the binding limit)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_per_view_dropin": dropin_e2e,
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         print(json.dumps(line))
     if world > 1:
@@ -388,6 +546,26 @@ def run_e2e(sc, vol_h, args, dev):
                     "layouts, pinned)"}
 
 
+def _fan2d_reference():
+    """FP64 reference projections for the fan2d workload's parity check."""
+    from oracle import oracle
+    orc = oracle.get("ref" if oracle.ref_available() else "port")
+
+    def ref(kind, v, img, sc, table, lf):
+        img = np.ascontiguousarray(img, dtype=np.float64)
+        if kind == "fb2d":
+            out = np.zeros(sc.nv)
+            orc.p2d("FB2D", out, img, sc, v, 0, table)
+            return out
+        lf = dict(lf)
+        beta = lf.pop("beta")
+        out = np.zeros(lf["detectorDimension"])
+        orc.lf2d("direct", oracle.LF2DParams(**lf), beta, 0.0, img, out, 1)
+        return out
+
+    return ref
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -398,9 +576,11 @@ def main(argv=None):
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-parity", action="store_true")
+    ap.add_argument("--skip-dense", action="store_true")
     ap.add_argument("--workload", default="pair3d",
                     choices=["pair3d", "parallel2d_recon", "fan2d", "cone3d_recon", "gates4d",
-                             "learned_warmstart", "learned_eval"],
+                             "learned_warmstart", "learned_eval", "projector_case", "unet_case"],
                     help="pair3d (default) is the benchmark line; the others measure the "
                          "remaining configurations (yoricktrtt_b200/workloads.py)")
     ap.add_argument("--param", action="append", default=[], metavar="KEY=VALUE",
@@ -421,6 +601,8 @@ def main(argv=None):
                 kw[k] = json.loads(v)
             except ValueError:
                 kw[k] = v
+        if args.workload == "fan2d":
+            kw["reference"] = _fan2d_reference()
         res = getattr(workloads, args.workload)(**kw)
         print(json.dumps({"workload": args.workload, **res}))
         return 0

@@ -358,11 +358,10 @@ int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, fl
 
 /* Allocation-free cone-beam direct projector.  No counterpart in the
  * reference (whose plugin allocates on the host per voxel).  For callers that
- * cannot call cudaMalloc: code running while a stream is captured into a
- * CUDA graph, real-time or embedded hosts that forbid device allocation after
- * start-up (cudaMalloc may synchronise the device), and frameworks whose
- * device memory belongs to their own pool allocator.  Same result as
- * trtt_b200_plan3d_forward with the closed-form cubic footprint and
+ * cannot call cudaMalloc: real-time or embedded hosts that forbid device
+ * allocation after start-up (cudaMalloc may synchronise the device), and
+ * frameworks whose device memory belongs to their own pool allocator.  Same
+ * sizes accepted and same result as trtt_b200_plan3d_forward with the closed-form cubic footprint and
  * TRTT_B200_LAYOUT_COLUMNS: sino[view][nv][nu] += H_view vol_columns for
  * nviews cone-beam views (xos/xsd: host, nviews*12).  vol_columns and sino are
  * device arrays owned by the caller.  The per-view geometry lives in one
@@ -370,7 +369,7 @@ int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, fl
  * held by every GPU that loads the library until exit); more views return -1.
  * Every call reuses that array, so calls overlapping on the GPU race; host
  * threads are serialised and the call returns after the projection has
- * completed.  The first call on a device looks the array up
+ * completed (it waits for `stream`).  The first call on a device looks the array up
  * (cudaGetSymbolAddress): make it before any stream capture. */
 #define TRTT_B200_NOALLOC_MAX_VIEWS 2048
 int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, float *sino,

@@ -27,7 +27,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "liboracle_ref.so")
-REFROOT = "/root/reference"
+# reference checkout (read-only): $TRTT_REFERENCE_ROOT, else the mounted tree
+REFROOT = os.environ.get("TRTT_REFERENCE_ROOT", "/root/reference")
 
 _dp = C.POINTER(C.c_double)
 _lp = C.POINTER(C.c_long)
@@ -69,7 +70,7 @@ def build(ref: bool = False) -> None:
     compiled reference) with oracle/Makefile."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REFROOT):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFROOT={REFROOT}"], check=True)
 
 
 def _dptr(a):

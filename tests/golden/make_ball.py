@@ -9,6 +9,8 @@ the phantom file and the image verbatim and keeps every 45th projection
 
     python tests/golden/make_ball.py [reference_root]
 
+(reference_root defaults to $TRTT_REFERENCE_ROOT, else /root/reference).
+
 Outputs: tests/golden/ball/{boule.obj, boule.data, proj_boule_every45.data}.
 """
 import os
@@ -21,7 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 EVERY = 45
 
 
-def main(root="/root/reference"):
+def main(root=None):
+    root = root or os.environ.get("TRTT_REFERENCE_ROOT", "/root/reference")
     src = os.path.join(root, "Tomography_3D", "Simul_Data")
     dst = os.path.join(HERE, "ball")
     os.makedirs(dst, exist_ok=True)

@@ -66,10 +66,8 @@ extern "C" int trtt_b200_plan3d_create(trtt_b200_plan3d **plan, int geometry,
   *plan = nullptr;
   const int g = geom_code(geometry);
   if (g < 0) return fail("plan3d_create: geometry must be 3 (parallel), 4 (cone) or 5 (fan)");
-  if (!dim_ok(nx) || !dim_ok(ny) || !dim_ok(nz) || !dim_ok(nu) || !dim_ok(nv) || !dim_ok(nviews))
-    return fail("plan3d_create: sizes must be in [1, 2^30)");
-  if (nx * ny >= (1L << 31) || nx * ny * nz >= (1L << 40))
-    return fail("plan3d_create: volume too large");
+  if (const char *why = check_sizes3d(nx, ny, nz, nu, nv, nviews))
+    return fail(std::string("plan3d_create: ") + why);
   if (!xos || !xsd) return fail("plan3d_create: null xos/xsd");
   if (cum_footprint && (size_footprint < 1 || !coord_footprint || !(step_footprint > 0)))
     return fail("plan3d_create: invalid footprint table");

@@ -98,6 +98,19 @@ inline Params3D make_params(int geom, long nx, long ny, long nz, double s_scl, i
   return P;
 }
 
+// Size limits shared by every 3D entry point that takes device arrays:
+// dimensions in [1, 2^30) (int indices in the kernels), one volume slice
+// below 2^31 voxels and the whole volume below 2^40.  Returns nullptr when
+// the sizes are accepted, else the reason.
+inline const char *check_sizes3d(long nx, long ny, long nz, long nu, long nv, long nviews)
+{
+  auto ok = [](long n) { return n >= 1 && n < (1L << 30); };
+  if (!ok(nx) || !ok(ny) || !ok(nz) || !ok(nu) || !ok(nv) || !ok(nviews))
+    return "sizes must be in [1, 2^30)";
+  if (nx * ny >= (1L << 31) || nx * ny * nz >= (1L << 40)) return "volume too large";
+  return nullptr;
+}
+
 // Band shape of the direct kernel for a detector nu cells wide.
 inline void choose_band(int nu, int nv, int &band_rows, int &warps)
 {

@@ -1,14 +1,14 @@
 // noalloc.cu -- allocation-free variant of the cone-beam direct projector.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is
-// being captured into a graph (allocation is not a capturable operation),
-// real-time or embedded hosts that forbid device allocation after start-up
-// (cudaMalloc can synchronise the whole device and stall other streams),
-// and frameworks whose memory is owned by their own pool allocator.  The
-// plan API allocates its per-view geometry table on the device; this entry
-// point instead keeps that table (and its error word) in one file-scope
-// device array, so the call allocates nothing.  The caller still passes the
-// input volume and the output detector stack.
+// Some callers cannot call cudaMalloc: real-time or embedded hosts that
+// forbid device allocation after start-up (cudaMalloc can synchronise the
+// whole device and stall the streams of other work), and frameworks whose
+// device memory belongs to their own pool allocator, which must not see a
+// library allocate behind its back.  The plan API allocates its per-view
+// geometry table on the device; this entry point instead keeps that table
+// (and its error word) in one file-scope device array, so the call
+// allocates nothing.  The caller still passes the input volume and the
+// output detector stack.
 //
 // Limits and sharing:
 //  * at most TRTT_B200_NOALLOC_MAX_VIEWS (2048) views per call, i.e. 2048
@@ -18,7 +18,8 @@
 //    the error word is cleared by each call), so calls that overlap on the
 //    GPU -- on two streams, or from two host threads -- race on it.  Host
 //    threads are serialised by a mutex and the call returns only after the
-//    projection has completed;
+//    projection has completed (it reads the error word back and waits for
+//    the stream);
 //  * the first call on each device looks the array's device address up
 //    (cudaGetSymbolAddress, which may load the module); make that first call
 //    before any stream capture begins.
@@ -60,12 +61,11 @@ extern "C" int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, fl
 {
   clear_error();
   if (!vol_columns || !sino || !xos || !xsd) return fail("cb3d_cubic_forward_noalloc: null argument");
-  if (!dim_ok(nx) || !dim_ok(ny) || !dim_ok(nz) || !dim_ok(nu) || !dim_ok(nv) || nviews < 1)
-    return fail("cb3d_cubic_forward_noalloc: dimensions out of range");
   if (nviews > kMaxViews)
     return fail("cb3d_cubic_forward_noalloc: at most " + std::to_string(kMaxViews) +
                 " views per call (the scratch array is static); got " + std::to_string(nviews));
-  if (nx * ny >= (1L << 31)) return fail("cb3d_cubic_forward_noalloc: volume too large");
+  if (const char *why = check_sizes3d(nx, ny, nz, nu, nv, nviews))
+    return fail(std::string("cb3d_cubic_forward_noalloc: ") + why);
   std::lock_guard<std::mutex> lock(g_mu);
   int dev = 0;
   TRTT_CK(cudaGetDevice(&dev));

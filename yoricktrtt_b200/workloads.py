@@ -89,67 +89,52 @@ def parallel2d_recon(iterations=50, seed=0):
             "rel_err_vs_phantom": err}
 
 
-def fan2d(sample_views=4, seed=0):
+def fan2d(sample_views=4, seed=0, reference=None):
+    """2D fan-beam throughput of the B-spline (closed-form and table) and
+    Long-Fessler pairs.  ``reference(kind, view, img, scan, table, lf)``, when
+    given, returns the FP64 reference projection of one view (the caller
+    supplies the checker; this package does not import one), and the result
+    then carries the largest relative L2 error over ``sample_views`` views."""
     torch = _torch()
-    from oracle import oracle  # checker only
     from . import dropin, footprint as F, geometry as G, phantoms as P
     from .recon import Projector2D, dot
     sc = G.circular_scan_2d(512, 512, 0.5, 3, 1024, 0.5, 720, mode=G.TRTT_FAN_BEAM,
                             rsc=1000.0, rsd=1500.0)
     img = P.ellipses_2d(512, 512, n=10, seed=seed)
     xt = torch.tensor(img, dtype=torch.float32, device="cuda")
-    orc = oracle.get("port")
     res = {"config": "2D fan 512^2, 720 views / 2 pi, 1024 bins, SID 1000, SDD 1500, 0.5 mm"}
     tab = F.make_footprint(3, 10001)
     views = np.linspace(0, 719, sample_views).astype(int)
-    for name, pr, ref_fn in [
-        ("bspline_cubic", Projector2D(sc), lambda v, out: orc.p2d("FB2D", out, img, sc, int(v), 0, None)),
-        ("bspline_table", Projector2D(sc, tab), lambda v, out: orc.p2d("FB2D", out, img, sc, int(v), 0, tab)),
-    ]:
-        y = torch.zeros(sc.nviews, sc.nv, device="cuda")
+    # Long-Fessler with the same geometry (Ytrtt_2D_projectors_Long_Fessler.i:216-233)
+    lf = dict(pixelSize=0.5, pixelStep=0.5, voxelSize=0.5, sourceDistance=1000.0,
+              detectorDistance=500.0, objectOffset1=0.0, objectOffset2=0.0,
+              objectDimension1=512, objectDimension2=512, detectorDimension=1024)
+    beta = sc.theta - math.pi / 2
+    cases = [("bspline_cubic", Projector2D(sc), None, sc.nv),
+             ("bspline_table", Projector2D(sc, tab), tab, sc.nv),
+             ("long_fessler", Projector2D(lf_params=dropin.LF2DParams(**lf), beta=beta,
+                                          offset=np.zeros(sc.nviews)), None, 1024)]
+    for name, pr, table, nbins in cases:
+        y = torch.zeros(sc.nviews, nbins, device="cuda")
         b = torch.zeros_like(xt)
         tf = _time(lambda: pr.forward(xt, out=y.zero_()))
         yy = torch.rand_like(y)
         tb = _time(lambda: pr.backward(yy, out=b.zero_()))
         pr.forward(xt, out=y.zero_())
-        yh = y.double().cpu().numpy()
-        errs = []
-        for v in views:
-            ref = np.zeros(sc.nv)
-            ref_fn(v, ref)
-            errs.append(float(np.linalg.norm(yh[v] - ref) / np.linalg.norm(ref)))
         pr.backward(yy, out=b.zero_())
         adj = abs(dot(y, yy) - dot(xt, b)) / (math.sqrt(dot(y, y)) * math.sqrt(dot(yy, yy)))
-        res[name] = {"fwd_ms": tf, "back_ms": tb, "projections_per_s": 2 * sc.nviews / ((tf + tb) / 1e3),
-                     "max_rel_l2_vs_fp64": max(errs), "adjoint_rel": adj}
-    # Long-Fessler with the same geometry (Ytrtt_2D_projectors_Long_Fessler.i:216-233)
-    lfp = dropin.LF2DParams(pixelSize=0.5, pixelStep=0.5, voxelSize=0.5, sourceDistance=1000.0,
-                            detectorDistance=500.0, objectOffset1=0.0, objectOffset2=0.0,
-                            objectDimension1=512, objectDimension2=512, detectorDimension=1024)
-    from oracle.oracle import LF2DParams as OP
-    olp = OP(pixelSize=0.5, pixelStep=0.5, voxelSize=0.5, sourceDistance=1000.0,
-             detectorDistance=500.0, objectOffset1=0.0, objectOffset2=0.0,
-             objectDimension1=512, objectDimension2=512, detectorDimension=1024)
-    beta = sc.theta - math.pi / 2
-    offs = np.zeros(sc.nviews)
-    pr = Projector2D(lf_params=lfp, beta=beta, offset=offs)
-    y = torch.zeros(sc.nviews, 1024, device="cuda")
-    b = torch.zeros_like(xt)
-    tf = _time(lambda: pr.forward(xt, out=y.zero_()))
-    yy = torch.rand_like(y)
-    tb = _time(lambda: pr.backward(yy, out=b.zero_()))
-    pr.forward(xt, out=y.zero_())
-    yh = y.double().cpu().numpy()
-    errs = []
-    for v in views:
-        ref = np.zeros(1024)
-        orc.lf2d("direct", olp, beta[v], 0.0, img, ref, 1)
-        errs.append(float(np.linalg.norm(yh[v] - ref) / np.linalg.norm(ref)))
-    pr.backward(yy, out=b.zero_())
-    adj = abs(dot(y, yy) - dot(xt, b)) / (math.sqrt(dot(y, y)) * math.sqrt(dot(yy, yy)))
-    res["long_fessler"] = {"fwd_ms": tf, "back_ms": tb,
-                           "projections_per_s": 2 * sc.nviews / ((tf + tb) / 1e3),
-                           "max_rel_l2_vs_fp64": max(errs), "adjoint_rel": adj}
+        r = {"fwd_ms": tf, "back_ms": tb, "projections_per_s": 2 * sc.nviews / ((tf + tb) / 1e3),
+             "adjoint_rel": adj}
+        if reference is not None:
+            yh = y.double().cpu().numpy()
+            errs = []
+            for v in views:
+                ref = reference("lf" if name == "long_fessler" else "fb2d", int(v), img, sc, table,
+                                dict(lf, beta=float(beta[v])))
+                errs.append(float(np.linalg.norm(yh[v] - ref) / np.linalg.norm(ref)))
+            r["max_rel_l2_vs_fp64"] = max(errs)
+            r["sample_views"] = [int(v) for v in views]
+        res[name] = r
     return res
 
 
@@ -280,3 +265,76 @@ def learned_eval(weights=None, n_test=20, eval_maxiter=500, ref_maxiter=600, see
     return {"config": f"learned warm start evaluation ({os.path.basename(weights)}): {n_test} held-out "
                       f"seeds, 128^3, 90 views, 256^2, Poisson I0=1e4, VMLM-B + TV to 1e-6",
             "summary": summarize(rows), "per_seed": rows}
+
+
+def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps=1, dense=0,
+                   tiles=None, seed=0):
+    """One cone-beam projector case for profiling: an n x n x nz volume of 20
+    ellipsoids (``dense=1`` adds a positive floor so that every voxel is
+    non-zero), ``views`` views on an nd x nd detector, SID 1000 mm, SDD
+    1500 mm, closed-form cubic footprint, columns layout.  Runs ``reps``
+    direct and/or transpose launches, checks the status flag and returns the
+    CUDA-event time of the last launch of each direction.  ``tiles`` is a
+    set_tiles() argument list."""
+    torch = _torch()
+    from . import geometry as G, phantoms as P
+    from .projectors import Projector3D, columns_from_xyz
+    nz = nz or n
+    sc = G.circular_scan_3d(n, n, nz, 1.0, 3, nd, nd, 1.0, 1.0, views, rsc=1000.0, rsd=1500.0)
+    vol = P.ellipsoids_3d(n, n, nz, n=20, seed=seed, dtype=np.float32)
+    if dense:
+        vol = vol + np.float32(0.05)
+    pr = Projector3D(sc)
+    if tiles:
+        pr.set_tiles(*tiles)
+    x = columns_from_xyz(torch.tensor(vol, device="cuda"))
+    y = torch.zeros(pr.detector_shape(), device="cuda")
+    b = torch.zeros_like(x)
+    res = {"config": f"cone {n}x{n}x{nz} -> {views} x {nd}^2, cubic, {'dense' if dense else 'phantom'}"}
+    for _ in range(reps):
+        if direct:
+            a, e = _events()
+            a.record()
+            pr.forward(x, out=y.zero_(), layout="columns")
+            e.record()
+            torch.cuda.synchronize()
+            res["direct_ms"] = a.elapsed_time(e)
+        if transpose:
+            a, e = _events()
+            a.record()
+            pr.backward(y if direct else torch.ones_like(y), out=b.zero_(), layout="columns")
+            e.record()
+            torch.cuda.synchronize()
+            res["transpose_ms"] = a.elapsed_time(e)
+    pr.status()
+    res["voxel_views"] = n * n * nz * views
+    return res
+
+
+def unet_case(size=128, batch=1, reps=1, train=1, seed=0):
+    """One U-Net case for profiling the tensor-core convolutions: ``reps``
+    forward passes (and training steps when ``train``) on a batch of
+    size^3 inputs; returns the CUDA-event time of the last of each."""
+    torch = _torch()
+    from .unet import UNet3D
+    net = UNet3D(seed=seed)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.rand(batch, size, size, size, device="cuda", generator=g)
+    t = torch.rand(batch, size, size, size, device="cuda", generator=g)
+    res = {"config": f"U-Net 3 levels 16/32/64, batch {batch} x {size}^3"}
+    for _ in range(reps):
+        a, e = _events()
+        a.record()
+        net.forward(x)
+        e.record()
+        torch.cuda.synchronize()
+        res["forward_ms"] = a.elapsed_time(e)
+        if train:
+            a, e = _events()
+            a.record()
+            net.train_step(x, t)
+            e.record()
+            torch.cuda.synchronize()
+            res["train_step_ms"] = a.elapsed_time(e)
+    net.status()
+    return res
