@@ -218,6 +218,29 @@ int trtt_b200_plan3d_set_columns(trtt_b200_plan3d *plan, int cols);
 /* 1 if every view of the plan uses the column-factorised kernels. */
 int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
 
+/* Orbit symmetry.  No counterpart in the reference.  At creation a plan of
+ * the closed-form model whose views are all column-factorised groups its
+ * views by turns of the volume grid about the z axis: {a, b1, b2, b3} when
+ * view b_m sees voxel (i, j, k) where view a sees (R^m(i, j), k), R the
+ * quarter turn (i, j) -> (n-1-j, i) of a square grid of even side (a
+ * circular orbit of 4N views over 2 pi), else {a, b2} for the half turn (nx
+ * or ny even), else {a}; xsd equal within 1e-10.  A whole-scan projection of
+ * a one-gate plan then evaluates the footprints of each group's first view
+ * once for all members (group kernels).  counts[0..2] = singles, pairs and
+ * quads found (all-zero when the group kernels never apply to the plan).
+ * set_symmetry(plan, 0) returns to the per-view kernels (results equal to
+ * FP32 summation order). */
+int trtt_b200_plan3d_groups(const trtt_b200_plan3d *plan, long *counts);
+int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *plan, int on);
+
+/* Group-kernel shape: detector-row band heights of the direct kernel for
+ * groups of 4, 2 and 1 views (0 keeps the current value; each in [2, nv]
+ * and within shared memory) and the detector bytes the transpose covers per
+ * launch (0 keeps; the images of one launch stay in L2 while every column
+ * orbit walks them). */
+int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *plan, int band_rows4, int band_rows2,
+                                     int band_rows1, long back_chunk_bytes);
+
 /* shape[0..6] = nx, ny, nz, nu, nv, nviews, number of gates. */
 int trtt_b200_plan3d_shape(const trtt_b200_plan3d *plan, long *shape);
 

@@ -55,6 +55,9 @@ SIGNATURES = {
     "trtt_b200_plan3d_set_tiles": (_I, [_vp, _I, _I]),
     "trtt_b200_plan3d_factorized": (_I, [_vp]),
     "trtt_b200_plan3d_set_columns": (_I, [_vp, _I]),
+    "trtt_b200_plan3d_groups": (_I, [_vp, _vp]),
+    "trtt_b200_plan3d_set_symmetry": (_I, [_vp, _I]),
+    "trtt_b200_plan3d_set_group_tiles": (_I, [_vp, _I, _I, _I, _L]),
     "trtt_b200_plan3d_destroy": (_I, [_vp]),
     "trtt_b200_plan2d_create": (_I, [C.POINTER(_vp), _I, _L, _L, _D, _I, _dp, _L, _D, _dp, _L,
                                       _D, _L, _dp, _dp]),

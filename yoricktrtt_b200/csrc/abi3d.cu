@@ -5,9 +5,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "host3d.h"
@@ -33,7 +35,26 @@ struct trtt_b200_plan3d {
   bool factorized = true;
   DevBuf views, cum, gate_ptr, entries, scratch, err;
   std::vector<View3D> hviews;
+  // view groups related by turns of the grid (closed-form model, factorised
+  // views): index 0 singles, 1 pairs (half turns), 2 quads (quarter turns)
+  bool sym = true;        // use the group kernels when they apply
+  bool grouped = false;   // groups were found (some group has 2 or 4 views)
+  int ngroups[3] = {0, 0, 0};
+  DevBuf groups[3];
+  int gband[3] = {64, 32, 32};  // direct: band rows per group size
+  long back_chunk_bytes = 32L << 20;  // transpose: detector bytes per launch
 };
+
+static int group_size_of(int idx) { return idx == 2 ? 4 : idx + 1; }
+
+// Group kernels apply: closed-form model, every view factorised, one gate,
+// the whole scan in one call.
+static bool use_groups(const trtt_b200_plan3d *pl, long view0, long nview)
+{
+  return pl->sym && pl->grouped && pl->factorized && pl->P.model == MODEL_CUBIC && pl->nt == 1 &&
+         !pl->pull && !pl->tc && pl->cols == 1 && view0 == 0 && nview == pl->nviews &&
+         pl->nviews <= 65535;
+}
 
 static int upload_gates(trtt_b200_plan3d *pl, const std::vector<std::vector<GateEntry>> &lists)
 {
@@ -93,6 +114,23 @@ extern "C" int trtt_b200_plan3d_create(trtt_b200_plan3d **plan, int geometry,
     if (!pl->hviews[v].factorized) pl->factorized = false;
   }
   choose_band(pl->P.nu, pl->P.nv, pl->band_rows, pl->warps);
+  if (pl->factorized && !cum_footprint) {
+    std::vector<int> lists[3];
+    find_view_groups(nx, ny, nviews, xos, xsd, lists);
+    pl->grouped = !lists[1].empty() || !lists[2].empty();
+    for (int q = 0; q < 3 && pl->grouped; ++q) {
+      pl->ngroups[q] = (int)(lists[q].size() / 4);
+      if (lists[q].empty()) continue;
+      cudaError_t eg = pl->groups[q].ensure(sizeof(int) * lists[q].size());
+      if (eg == cudaSuccess)
+        eg = cudaMemcpy(pl->groups[q].p, lists[q].data(), sizeof(int) * lists[q].size(),
+                        cudaMemcpyHostToDevice);
+      if (eg != cudaSuccess) {
+        delete pl;
+        return fail_cuda(eg, "plan3d_create(groups)");
+      }
+    }
+  }
   cudaError_t e = pl->views.ensure(sizeof(View3D) * nviews);
   if (e == cudaSuccess)
     e = cudaMemcpy(pl->views.p, pl->hviews.data(), sizeof(View3D) * nviews, cudaMemcpyHostToDevice);
@@ -199,6 +237,45 @@ extern "C" int trtt_b200_plan3d_set_columns(trtt_b200_plan3d *pl, int cols)
   return 0;
 }
 
+extern "C" int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *pl, int on)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_symmetry: null plan");
+  pl->sym = on != 0;
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_groups(const trtt_b200_plan3d *pl, long *counts)
+{
+  clear_error();
+  if (!pl || !counts) return fail("plan3d_groups: null argument");
+  for (int q = 0; q < 3; ++q) counts[q] = pl->grouped ? pl->ngroups[q] : 0;
+  if (!pl->grouped) counts[0] = pl->factorized && pl->P.model == MODEL_CUBIC ? pl->nviews : 0;
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *pl, int band_rows4, int band_rows2,
+                                                int band_rows1, long back_chunk_bytes)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_group_tiles: null plan");
+  const int req[3] = {band_rows1, band_rows2, band_rows4};
+  const int usplit = (pl->P.nu + 255) / 256;
+  const int utile = (pl->P.nu + usplit - 1) / usplit;
+  for (int q = 0; q < 3; ++q) {
+    if (req[q] == 0) continue;
+    if (req[q] < 2) return fail("plan3d_set_group_tiles: band rows must be >= 2");
+    const int r = std::min(req[q], pl->P.nv);
+    if (group_fwd_smem(group_size_of(q), r, utile, 16) > 227u * 1024u)
+      return fail("plan3d_set_group_tiles: band does not fit in shared memory");
+  }
+  for (int q = 0; q < 3; ++q)
+    if (req[q]) pl->gband[q] = req[q];
+  if (back_chunk_bytes < 0) return fail("plan3d_set_group_tiles: negative chunk size");
+  if (back_chunk_bytes) pl->back_chunk_bytes = back_chunk_bytes;
+  return 0;
+}
+
 extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
 {
   return pl && pl->factorized ? 1 : 0;
@@ -244,7 +321,55 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
       volo = pl->scratch.as<float>();
     }
   }
-  if (forward) {
+  if (forward && use_groups(pl, view0, nview)) {
+    for (int q = 2; q >= 0; --q) {
+      if (!pl->ngroups[q]) continue;
+      const int G = group_size_of(q);
+      GroupFwdLaunch L;
+      L.P = P;
+      L.views = pl->views.as<View3D>();
+      L.groups = pl->groups[q].as<int>();
+      L.ngroups = pl->ngroups[q];
+      L.vol = volc;
+      L.sino = dst;
+      L.sino_view_stride = npix;
+      L.band_rows = std::min(pl->gband[q], P.nv);
+      L.usplit = (P.nu + 255) / 256;
+      L.utile = (P.nu + L.usplit - 1) / L.usplit;
+      L.warps = 16;
+      L.err = pl->err.as<int>();
+      TRTT_CK(launch_fwd3d_group(L, G, st));
+      count_launch();
+    }
+  } else if (!forward && use_groups(pl, view0, nview)) {
+    for (int q = 2; q >= 0; --q) {
+      if (!pl->ngroups[q]) continue;
+      const int G = group_size_of(q);
+      GroupBackLaunch L;
+      L.P = P;
+      L.views = pl->views.as<View3D>();
+      L.groups = pl->groups[q].as<int>();
+      L.norbits = group_orbits(G, P.nx, P.ny);
+      L.sino = src;
+      L.sino_view_stride = npix;
+      L.vol = volo;
+      L.err = pl->err.as<int>();
+      // groups per launch: the launch's detector images stay in L2 while
+      // every orbit walks them
+      const long per_group = (long)G * npix * (long)sizeof(float);
+      const int chunk = (int)std::max<long>(1, pl->back_chunk_bytes / per_group);
+      for (int g0 = 0; g0 < pl->ngroups[q]; g0 += chunk) {
+        L.g_lo = g0;
+        L.g_hi = std::min(g0 + chunk, pl->ngroups[q]);
+        TRTT_CK(launch_back3d_group(L, G, st));
+        count_launch();
+      }
+    }
+    if (layout == TRTT_B200_LAYOUT_XYZ) {
+      TRTT_CK(col_f32_add_to_xyz_f32(volo, dst, P.nx, P.ny, P.nz, pl->nt, st));
+      count_launch();
+    }
+  } else if (forward) {
     Fwd3DLaunch L;
     L.P = P;
     L.views = pl->views.as<View3D>() + view0;
@@ -318,6 +443,7 @@ extern "C" int trtt_b200_plan3d_destroy(trtt_b200_plan3d *pl)
   pl->cum.release();
   pl->gate_ptr.release();
   pl->entries.release();
+  for (auto &gb : pl->groups) gb.release();
   pl->scratch.release();
   pl->err.release();
   delete pl;
@@ -363,6 +489,142 @@ std::vector<long> back_chunks(long nviews, long head, long full, int cap)
     size = std::min<double>(size * 1.5, (double)std::max<long>(1, full));
   }
   return b;
+}
+
+// Runs [first, last) of consecutive view indices among the members of
+// groups [g0, g1) of a list of groups of G views (4 ints per group).
+void member_runs(const std::vector<int> &list, int G, long g0, long g1,
+                 std::vector<std::pair<long, long>> &runs)
+{
+  std::vector<long> v;
+  for (long g = g0; g < g1; ++g)
+    for (int m = 0; m < G; ++m) v.push_back(list[4 * g + m]);
+  std::sort(v.begin(), v.end());
+  runs.clear();
+  for (size_t t = 0; t < v.size();) {
+    size_t e = t + 1;
+    while (e < v.size() && v[e] == v[e - 1] + 1) ++e;
+    runs.push_back({v[t], v[e - 1] + 1});
+    t = e;
+  }
+}
+
+// Host-buffer projection of a grouped scan (closed-form model, factorised
+// views, groups found by find_view_groups): the group kernels run in chunks
+// of groups; the forward reads each chunk's views back while later chunks
+// are projected, the transpose projects each chunk as soon as its views are
+// on the device.  `out64` already receives `out` (or zeros) on the copy
+// stream, ordered after ev[0].
+int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
+                   const std::vector<int> (&lists)[3], long nviews, int job,
+                   const std::function<cudaError_t(cudaStream_t)> &out_to_device)
+{
+  cudaStream_t st = D.stream, cp = D.copy, ks2 = D.stream2;
+  const long nx = P.nx, ny = P.ny, nz = P.nz, nu = P.nu, nv = P.nv;
+  const long nvox = nx * ny * nz, nview_px = nu * nv, npix = nview_px * nviews;
+  // group lists on the device, one after the other
+  long total = 0, offs[3];
+  for (int q = 0; q < 3; ++q) {
+    offs[q] = total;
+    total += (long)lists[q].size();
+  }
+  TRTT_CK(D.grp.ensure(sizeof(int) * std::max<long>(1, total)));
+  for (int q = 0; q < 3; ++q)
+    if (!lists[q].empty())
+      TRTT_CK(cudaMemcpyAsync(D.grp.as<int>() + offs[q], lists[q].data(), sizeof(int) * lists[q].size(),
+                              cudaMemcpyHostToDevice, st));
+  const int usplit = (int)((nu + 255) / 256), utile = (int)((nu + usplit - 1) / usplit);
+  std::vector<std::pair<long, long>> runs;
+  int ev = 2;
+  if (job == 0) {
+    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nvox, cudaMemcpyHostToDevice, st));
+    TRTT_CK(out_to_device(cp));
+    TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
+    TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
+    TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvents - 2], st));
+    TRTT_CK(cudaStreamWaitEvent(ks2, D.ev[DropIn::kEvents - 2], 0));
+    int unit = 0;
+    for (int q = 2; q >= 0; --q) {
+      const long n = (long)lists[q].size() / 4;
+      if (!n) continue;
+      const int G = q == 2 ? 4 : q + 1;
+      GroupFwdLaunch L;
+      L.P = P;
+      L.views = D.geom.as<View3D>();
+      L.vol = D.vol32.as<float>();
+      L.sino = D.det32.as<float>();
+      L.sino_view_stride = nview_px;
+      L.band_rows = (int)std::min<long>(G == 1 ? 64 : 32, nv);
+      L.usplit = usplit;
+      L.utile = utile;
+      L.warps = 16;
+      L.err = D.err.as<int>();
+      const long bands = (nv + L.band_rows - 1) / L.band_rows;
+      const long per_wave = (long)D.sms * (G == 4 ? 1 : 2);
+      const std::vector<long> cb = fwd_chunks(n, (n + 5) / 6, std::max<long>(1, per_wave / (bands * usplit)), 10);
+      for (size_t c = 0; c + 1 < cb.size(); ++c, ++unit) {
+        cudaStream_t ks = (unit & 1) ? ks2 : st;
+        L.groups = D.grp.as<int>() + offs[q] + 4 * cb[c];
+        L.ngroups = (int)(cb[c + 1] - cb[c]);
+        TRTT_CK(launch_fwd3d_group(L, G, ks));
+        TRTT_CK(cudaEventRecord(D.ev[ev], ks));
+        TRTT_CK(cudaStreamWaitEvent(cp, D.ev[ev], 0));
+        ++ev;
+        count_launch();
+        member_runs(lists[q], G, cb[c], cb[c + 1], runs);
+        for (const auto &r : runs) {
+          const long off = r.first * nview_px, cnt = (r.second - r.first) * nview_px;
+          TRTT_CK(f32_add_to_f64(D.det32.as<float>() + off, D.out64.as<double>() + off, cnt, cp));
+          TRTT_CK(cudaMemcpyAsync(out + off, D.out64.as<double>() + off, sizeof(double) * cnt,
+                                  cudaMemcpyDeviceToHost, cp));
+          count_launch();
+        }
+      }
+    }
+    TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvents - 1], ks2));
+    TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvents - 1], 0));
+    TRTT_CK(cudaEventRecord(D.ev[1], cp));
+    TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
+    TRTT_CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  // transpose: views arrive in chunks of groups on the copy stream
+  TRTT_CK(cudaMemsetAsync(D.vol32.p, 0, sizeof(float) * nvox, st));
+  for (int q = 2; q >= 0; --q) {
+    const long n = (long)lists[q].size() / 4;
+    if (!n) continue;
+    const int G = q == 2 ? 4 : q + 1;
+    GroupBackLaunch L;
+    L.P = P;
+    L.views = D.geom.as<View3D>();
+    L.groups = D.grp.as<int>() + offs[q];
+    L.norbits = group_orbits(G, (int)nx, (int)ny);
+    L.sino = D.det32.as<float>();
+    L.sino_view_stride = nview_px;
+    L.vol = D.vol32.as<float>();
+    L.err = D.err.as<int>();
+    const std::vector<long> cb = back_chunks(n, std::max<long>(1, n / 32), (n + 5) / 6, 10);
+    for (size_t c = 0; c + 1 < cb.size(); ++c) {
+      member_runs(lists[q], G, cb[c], cb[c + 1], runs);
+      for (const auto &r : runs) {
+        const long off = r.first * nview_px, cnt = (r.second - r.first) * nview_px;
+        TRTT_CK(cudaMemcpyAsync(D.in64.as<double>() + off, in + off, sizeof(double) * cnt,
+                                cudaMemcpyHostToDevice, cp));
+        TRTT_CK(f64_to_f32(D.in64.as<double>() + off, D.det32.as<float>() + off, cnt, cp));
+        count_launch();
+      }
+      TRTT_CK(cudaEventRecord(D.ev[ev], cp));
+      TRTT_CK(cudaStreamWaitEvent(st, D.ev[ev], 0));
+      ++ev;
+      L.g_lo = (int)cb[c];
+      L.g_hi = (int)cb[c + 1];
+      TRTT_CK(launch_back3d_group(L, G, st));
+      count_launch();
+    }
+  }
+  TRTT_CK(out_to_device(cp));
+  TRTT_CK(cudaEventRecord(D.ev[1], cp));
+  return 1;  // continue with the common tail (error check, out += volume)
 }
 
 int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
@@ -419,7 +681,30 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     if (accumulate) return cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);
     return cudaMemsetAsync(D.out64.p, 0, sizeof(double) * nout, s);
   };
-  if (job == 0 && fact) {
+  std::vector<int> glists[3];
+  bool grouped = false;
+  if (fact && !cum && nviews <= 65535) {
+    find_view_groups(nx, ny, nviews, xos, xsd, glists);
+    grouped = !glists[1].empty() || !glists[2].empty();
+  }
+  if (grouped && job == 0) {
+    // the source-plane pre-check of the per-view path below, then the group
+    // kernels
+    TRTT_CK(launch_check_columns(P, D.geom.as<View3D>(), (int)nviews, D.err.as<int>(), st));
+    count_launch();
+    int herr = 0;
+    TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRTT_CK(cudaStreamSynchronize(st));
+    if (herr & TRTT_ERR_SOURCE_PLANE) {
+      std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
+      return fail("a voxel lies in the source plane (wk == 0)");
+    }
+    return host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device);
+  }
+  if (grouped) {
+    const int r = host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device);
+    if (r < 0) return r;
+  } else if (job == 0 && fact) {
     // Column-factorised views: the only failure (a voxel in the source
     // plane) is a property of the column geometry, so it is checked first;
     // the projection then runs in view chunks (fwd_chunks) and each chunk's
@@ -478,8 +763,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
     TRTT_CK(cudaStreamSynchronize(st));
     return 0;
-  }
-  if (job == 0) {
+  } else if (job == 0) {
     TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));

@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "kernels.h"
 #include "trtt_b200.h"
@@ -109,6 +110,93 @@ inline const char *check_sizes3d(long nx, long ny, long nz, long nu, long nv, lo
     return "sizes must be in [1, 2^30)";
   if (nx * ny >= (1L << 31) || nx * ny * nz >= (1L << 40)) return "volume too large";
   return nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Orbit symmetry of a scan's views.  R(i, j) = (n-1-j, i) is the quarter turn
+// of a square grid about the z axis, R^2(i, j) = (nx-1-i, ny-1-j) the half
+// turn of any grid.  View b is the m-turn image of view a when it sees voxel
+// (i, j, k) where view a sees voxel (R^m(i, j), k): its xos rows (p, q, r, s)
+// acting as p i + q j + r k + s equal those of view a with the substitution
+// applied, and its xsd equals view a's.  The footprints of view b's voxel
+// column c are then view a's footprints of column R^m(c), so a group of
+// views needs the footprint arithmetic of its first view only.
+// ---------------------------------------------------------------------------
+inline void turn_xos(const double *x, int m, long nx, long ny, double *out)
+{
+  for (int r = 0; r < 3; ++r) {
+    const double a = x[4 * r], b = x[4 * r + 1], c = x[4 * r + 2], d = x[4 * r + 3];
+    double *o = out + 4 * r;
+    o[2] = c;
+    if (m == 1) {
+      o[0] = b; o[1] = -a; o[3] = d + a * (double)(nx - 1);
+    } else if (m == 2) {
+      o[0] = -a; o[1] = -b; o[3] = d + a * (double)(nx - 1) + b * (double)(ny - 1);
+    } else if (m == 3) {
+      o[0] = -b; o[1] = a; o[3] = d + b * (double)(ny - 1);
+    } else {
+      o[0] = a; o[1] = b; o[3] = d;
+    }
+  }
+}
+
+// Rows of two 3x4 matrices equal within tol relative to the row's magnitude.
+inline bool coefs_match(const double *p, const double *q, double tol)
+{
+  for (int r = 0; r < 3; ++r) {
+    double s = 0.0;
+    for (int c = 0; c < 4; ++c) s = std::fmax(s, std::fmax(std::fabs(p[4 * r + c]), std::fabs(q[4 * r + c])));
+    for (int c = 0; c < 4; ++c)
+      if (!(std::fabs(p[4 * r + c] - q[4 * r + c]) <= tol * s)) return false;
+  }
+  return true;
+}
+
+// Greedy grouping in view order: {a, b1, b2, b3} (quarter turns, square grid
+// of even side), else {a, b2} (half turn, nx or ny even), else {a}.  Each
+// group is written as four view indices (unused slots -1) into the list of
+// its size: groups[0] singles, groups[1] pairs, groups[2] quads.
+inline void find_view_groups(long nx, long ny, long nviews, const double *xos, const double *xsd,
+                             std::vector<int> groups[3], double tol = 1e-10)
+{
+  std::vector<char> used(nviews, 0);
+  const bool quad_ok = nx == ny && nx % 2 == 0;
+  const bool pair_ok = nx % 2 == 0 || ny % 2 == 0;
+  auto find = [&](const double *coefs, const double *xd) -> long {
+    for (long b = 0; b < nviews; ++b)
+      if (!used[b] && coefs_match(xos + 12 * b, coefs, tol) && coefs_match(xsd + 12 * b, xd, tol))
+        return b;
+    return -1;
+  };
+  double t[12];
+  for (long a = 0; a < nviews; ++a) {
+    if (used[a]) continue;
+    used[a] = 1;
+    long mem[4] = {a, -1, -1, -1};
+    int n = 1;
+    if (quad_ok) {
+      long b[3];
+      for (int m = 1; m <= 3; ++m) {
+        turn_xos(xos + 12 * a, m, nx, ny, t);
+        b[m - 1] = find(t, xsd + 12 * a);
+      }
+      if (b[0] >= 0 && b[1] >= 0 && b[2] >= 0 && b[0] != b[1] && b[0] != b[2] && b[1] != b[2]) {
+        mem[1] = b[0]; mem[2] = b[1]; mem[3] = b[2];
+        n = 4;
+      }
+    }
+    if (n == 1 && pair_ok) {
+      turn_xos(xos + 12 * a, 2, nx, ny, t);
+      const long b2 = find(t, xsd + 12 * a);
+      if (b2 >= 0) {
+        mem[1] = b2;
+        n = 2;
+      }
+    }
+    for (int m = 1; m < n; ++m) used[mem[m]] = 1;
+    std::vector<int> &dst = groups[n == 4 ? 2 : n - 1];
+    for (int m = 0; m < 4; ++m) dst.push_back((int)mem[m]);
+  }
 }
 
 // Band shape of the direct kernel for a detector nu cells wide.

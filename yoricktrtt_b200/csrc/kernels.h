@@ -52,6 +52,44 @@ struct Back3DLaunch {
   int *err;
 };
 
+// Direct projector over groups of views related by turns of the volume grid
+// (proj3d_group.cu; closed-form model, column-factorised views, one gate).
+// `groups` holds 4 view indices per group (members m >= G unused); member m
+// sees at view groups[4g]'s footprint of column c the voxel column
+// R^{-t_m}(c) (t_m = m for G = 4, 2m for G = 2).
+struct GroupFwdLaunch {
+  Params3D P;
+  const View3D *views;   // device, all views of the plan
+  const int *groups;     // device, 4 * ngroups view indices
+  int ngroups;
+  const float *vol;      // column layout [j][i][k]
+  float *sino;           // [view][nv][nu], accumulated
+  long sino_view_stride;
+  int band_rows;         // R detector rows per CTA
+  int usplit, utile;     // u tiles per band and cells per tile (utile <= 256)
+  int warps;
+  int *err;
+};
+
+// Transpose over orbits of columns under the group's turns, for the groups
+// [g_lo, g_hi) of `groups`.
+struct GroupBackLaunch {
+  Params3D P;
+  const View3D *views;
+  const int *groups;
+  int g_lo, g_hi;
+  int norbits;           // group_orbits(G, nx, ny)
+  const float *sino;     // [view][nv][nu], all views of the plan
+  long sino_view_stride;
+  float *vol;            // column layout, accumulated
+  int *err;
+};
+
+size_t group_fwd_smem(int G, int band_rows, int utile, int warps);
+int group_orbits(int G, int nx, int ny);
+cudaError_t launch_fwd3d_group(const GroupFwdLaunch &L, int G, cudaStream_t st);
+cudaError_t launch_back3d_group(const GroupBackLaunch &L, int G, cudaStream_t st);
+
 cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st);
 cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st);
 // source-plane test of every column of column-factorised views (err |= flag)

@@ -45,7 +45,7 @@ struct DropIn {
   static constexpr int kChunks = 31;
   static constexpr int kEvents = kChunks + 4;
   cudaEvent_t ev[kEvents] = {};
-  DevBuf in64, out64, vol32, det32, geom, gates, aux, err;
+  DevBuf in64, out64, vol32, det32, geom, gates, aux, err, grp;
   cudaError_t init();
 };
 DropIn &dropin();

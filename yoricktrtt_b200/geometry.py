@@ -310,3 +310,82 @@ def gate_t_index(dates, tcycl: float, nt: int) -> np.ndarray:
     (Tomography_4D/Ytrtt4D_system.i:439-452): (t mod tcycl) * nt / tcycl."""
     t = np.asarray(dates, dtype=np.float64)
     return np.mod(t, tcycl) * (nt / tcycl)
+
+
+# ---------------------------------------------------------------------------
+# Orbit symmetry of a scan's views
+# ---------------------------------------------------------------------------
+def quarter_turn_coefs(xos, m: int, nx: int, ny: int) -> np.ndarray:
+    """xos coefficients of the view that sees voxel (i, j, k) where the view
+    with coefficients ``xos`` sees voxel (R^m(i, j), k), R the quarter turn
+    R(i, j) = (n-1-j, i) of a square nx = ny = n grid (m = 2, the half turn
+    (nx-1-i, ny-1-j), needs no square grid).  Each row (a, b, c, d) of the
+    3x4 matrix acts as a i + b j + c k + d."""
+    x = np.asarray(xos, dtype=np.float64).reshape(3, 4)
+    out = x.copy()
+    a, b = x[:, 0], x[:, 1]
+    if m == 1:
+        out[:, 0], out[:, 1], out[:, 3] = b, -a, x[:, 3] + a * (nx - 1)
+    elif m == 2:
+        out[:, 0], out[:, 1], out[:, 3] = -a, -b, x[:, 3] + a * (nx - 1) + b * (ny - 1)
+    elif m == 3:
+        out[:, 0], out[:, 1], out[:, 3] = -b, a, x[:, 3] + b * (ny - 1)
+    return out.reshape(12)
+
+
+def _coefs_match(p, q, tol):
+    p = np.asarray(p).reshape(3, 4)
+    q = np.asarray(q).reshape(3, 4)
+    scale = np.maximum(np.abs(p).max(axis=1), np.abs(q).max(axis=1))
+    return bool(np.all(np.abs(p - q) <= tol * np.maximum(scale, 1e-300)[:, None]))
+
+
+def view_groups(scan: "Scan3D", tol: float = 1e-10):
+    """Groups of views related by turns of the volume grid about the z axis:
+    [a, b1, b2, b3] when view b_m sees voxel (i, j, k) exactly where view a
+    sees voxel (R^m(i, j), k) for m = 1, 2, 3 (square grid of even side),
+    [a, b2] for the half turn alone (nx or ny even), [a] otherwise; xsd must
+    be equal within the group.  Greedy in view order.  Projecting a group
+    needs the footprints of view a only: view b_m's footprint of voxel
+    column c is view a's footprint of column R^m(c)."""
+    nx, ny, nv = scan.nx, scan.ny, scan.nviews
+    used = np.zeros(nv, dtype=bool)
+    groups = []
+    quad_ok = nx == ny and nx % 2 == 0
+    pair_ok = nx % 2 == 0 or ny % 2 == 0
+
+    def find(coefs, xsd):
+        for b in range(nv):
+            if not used[b] and _coefs_match(scan.xos[b], coefs, tol) and \
+                    _coefs_match(scan.xsd[b], xsd, tol):
+                return b
+        return -1
+
+    for a in range(nv):
+        if used[a]:
+            continue
+        used[a] = True
+        mem = [a]
+        if quad_ok:
+            b = [find(quarter_turn_coefs(scan.xos[a], m, nx, ny), scan.xsd[a]) for m in (1, 2, 3)]
+            if min(b) >= 0 and len(set(b)) == 3:
+                mem += b
+        if len(mem) == 1 and pair_ok:
+            b2 = find(quarter_turn_coefs(scan.xos[a], 2, nx, ny), scan.xsd[a])
+            if b2 >= 0:
+                mem.append(b2)
+        for b in mem[1:]:
+            used[b] = True
+        groups.append(mem)
+    return groups
+
+
+def turn_columns(i, j, m: int, nx: int, ny: int):
+    """(i, j) -> R^m(i, j), R(i, j) = (n-1-j, i); the half turn
+    R^2(i, j) = (nx-1-i, ny-1-j) also on a rectangular grid."""
+    m %= 4
+    if m == 2:
+        return nx - 1 - i, ny - 1 - j
+    for _ in range(m):
+        i, j = nx - 1 - j, i
+    return i, j

@@ -98,6 +98,23 @@ class Projector3D:
                    "trtt_b200_plan3d_set_tiles")
         _lib.check(lib.trtt_b200_plan3d_set_columns(self._h, cols), "trtt_b200_plan3d_set_columns")
 
+    def set_symmetry(self, on: bool = True) -> None:
+        """Use (default) or bypass the group kernels that share footprints
+        between views related by turns of the volume grid."""
+        _lib.check(_lib.load().trtt_b200_plan3d_set_symmetry(self._h, 1 if on else 0),
+                   "trtt_b200_plan3d_set_symmetry")
+
+    def groups(self):
+        """(singles, pairs, quads) of views the group kernels use."""
+        c = (C.c_long * 3)()
+        _lib.check(_lib.load().trtt_b200_plan3d_groups(self._h, c), "trtt_b200_plan3d_groups")
+        return tuple(int(x) for x in c)
+
+    def set_group_tiles(self, band_rows4=0, band_rows2=0, band_rows1=0, back_chunk_bytes=0):
+        _lib.check(_lib.load().trtt_b200_plan3d_set_group_tiles(
+            self._h, band_rows4, band_rows2, band_rows1, back_chunk_bytes),
+            "trtt_b200_plan3d_set_group_tiles")
+
     @property
     def factorized(self) -> bool:
         return bool(_lib.load().trtt_b200_plan3d_factorized(self._h))
