@@ -221,9 +221,13 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
-# names of the kernels the step launches (per direction), for the roofline
-FWD_KERNEL = "k_fwd3d_band_fast (direct, detector-row bands)"
-BACK_KERNEL = "k_back3d_col_fast (transpose, column gather)"
+# names of the kernels the step launches (per direction), for the roofline:
+# the group kernels when the scan's views group by turns of the grid, else
+# the per-view kernels
+KERNELS = {True: ("k_fwd3d_group (direct, view groups x detector-row bands)",
+                  "k_back3d_group (transpose, column orbits)"),
+           False: ("k_fwd3d_band_fast (direct, detector-row bands)",
+                   "k_back3d_col_fast (transpose, column gather)")}
 PARITY_VIEWS = (0, 137, 271)
 
 
@@ -364,6 +368,8 @@ def run_b200(args):
     pr = Projector3D(sc)
     if args.band_rows or args.warps:
         pr.set_tiles(args.band_rows, args.warps)
+    if args.no_symmetry:
+        pr.set_symmetry(False)
     vol_h = P.ellipsoids_3d(N, N, N, n=20, seed=0, dtype=np.float32)
     x = columns_from_xyz(torch.tensor(vol_h, device=dev))
     sino = torch.zeros(VIEWS, ND, ND, device=dev)
@@ -420,10 +426,12 @@ def run_b200(args):
     # bound by instruction issue, reported beside it from the committed ncu
     # instruction counts of the same kernels at this workload
     nvox, npix = N ** 3, ND * ND
+    grouped = pr.groups()[1] + pr.groups()[2] > 0 and not args.no_symmetry
+    fwd_kernel, back_kernel = KERNELS[grouped]
     if back_avg >= fwd_avg:
-        kern, kms = BACK_KERNEL, back_avg
+        kern, kms = back_kernel, back_avg
     else:
-        kern, kms = FWD_KERNEL, fwd_avg
+        kern, kms = fwd_kernel, fwd_avg
     alg_bytes = VIEWS * (4 * nvox + 4 * npix)
     peaks = {}
     try:
@@ -481,7 +489,10 @@ def run_b200(args):
                        "l2": "256 MiB buffer written between steps (inside the timed region); "
                              "the 360-view detector stack (377 MB) exceeds L2",
                        "fwd_ms": fwd_avg, "back_ms": back_avg,
-                       "band_rows": args.band_rows or "auto"},
+                       "band_rows": args.band_rows or "auto",
+                       "view_groups": {"singles": pr.groups()[0], "half_turn_pairs": pr.groups()[1],
+                                       "quarter_turn_quads": pr.groups()[2],
+                                       "used": bool(grouped)}},
             "parity": parity,
             "dense": dense,
             "roofline": {"bound": "issue", "kernel": kern, "achieved": achieved, "peak": peak,
@@ -578,6 +589,8 @@ def main(argv=None):
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-parity", action="store_true")
     ap.add_argument("--skip-dense", action="store_true")
+    ap.add_argument("--no-symmetry", action="store_true",
+                    help="per-view kernels even where views group by turns of the grid")
     ap.add_argument("--workload", default="pair3d",
                     choices=["pair3d", "parallel2d_recon", "fan2d", "cone3d_recon", "gates4d",
                              "learned_warmstart", "learned_eval", "projector_case", "unet_case"],
