@@ -87,6 +87,22 @@ int trtt_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
 int trtt_DD_PB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
                  long nu, long nv, double u_scl, double v_scl, double *xos,
                  double *xsd, int job);
+/* Replaces the reference's trtt_DD_CB3D, commented out and unfinished in
+ * plugin/trtt_3D_projectors.c:1340-1434 (same arguments as trtt_DD_PB3D):
+ * cone-beam distance-driven footprint completed with its intent (the voxel
+ * section through the centre, perpendicular to x or y, projected from the
+ * source through its four corners; its bounding detector rectangle clamped
+ * like trtt_DD_PB3D; weight s^3 magn^2 delta_u delta_v spread over the
+ * rectangle; the transpose is the adjoint).  FP64; 0 or -1 (a voxel centre
+ * in the source plane, out unchanged). */
+int trtt_DD_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+                 long nu, long nv, double u_scl, double v_scl, double *xos,
+                 double *xsd, int job);
+/* trtt_DD_CB3D over nviews views at once (xos/xsd: nviews*12 coefficients;
+ * out/in: nviews detector images of nv x nu doubles, view-major). */
+int trtt_b200_dd_cb3d(double *out, const double *in, long nx, long ny, long nz, double s_scl,
+                      long nu, long nv, double u_scl, double v_scl, long nviews,
+                      const double *xos, const double *xsd, int job);
 int trtt_PB3D_cubic(double *out, double *in, long nx, long ny, long nz,
                     double s_scl, int s_deg, long nu, long nv, double u_scl,
                     double v_scl, double *xos, double *xsd, int job);

@@ -47,9 +47,12 @@ _SIGS = {
     "PB3D": [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I],
     "CB3D": [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I],
     "DD_PB3D": [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _dp, _dp, _I],
+    # port only: the reference carries trtt_DD_CB3D commented out
+    "DD_CB3D": [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _dp, _dp, _I],
     "PB3D_cubic": [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I],
     "CB3D_cubic": [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I],
 }
+_PORT_ONLY = {"DD_CB3D"}
 _LF = ["direct", "line_integ_direct", "adjoint", "line_integ_adjoint"]
 _LFS = ["sparser", "line_integ_sparser"]
 
@@ -95,6 +98,8 @@ class Oracle:
         pre = "orc_" if kind == "port" else "trtt_"
         self._f = {}
         for name, sig in _SIGS.items():
+            if kind != "port" and name in _PORT_ONLY:
+                continue
             fn = getattr(self.lib, pre + name)
             fn.argtypes = sig
             fn.restype = C.c_int
@@ -149,6 +154,18 @@ class Oracle:
         _chk(out)
         _chk(vol)
         return self._f["DD_PB3D"](
+            _dptr(out), _dptr(vol), scan.nx, scan.ny, scan.nz, scan.s_scl,
+            scan.nu, scan.nv, scan.u_scl, scan.v_scl, _dptr(xos), _dptr(xsd),
+            job)
+
+    def dd_cb3d(self, out, vol, scan, view, job):
+        """Cone-beam distance-driven pair (the reference's unfinished
+        trtt_DD_CB3D, completed; port only)."""
+        xos = np.ascontiguousarray(scan.xos[view], dtype=np.float64)
+        xsd = np.ascontiguousarray(scan.xsd[view], dtype=np.float64)
+        _chk(out)
+        _chk(vol)
+        return self._f["DD_CB3D"](
             _dptr(out), _dptr(vol), scan.nx, scan.ny, scan.nz, scan.s_scl,
             scan.nu, scan.nv, scan.u_scl, scan.v_scl, _dptr(xos), _dptr(xsd),
             job)

@@ -65,6 +65,11 @@ int orc_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
 int orc_DD_PB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
                 long nu, long nv, double u_scl, double v_scl, double *xos,
                 double *xsd, int job);
+/* Cone-beam distance-driven pair: the reference's unfinished trtt_DD_CB3D
+ * (plugin/trtt_3D_projectors.c:1340-1434) completed with its intent. */
+int orc_DD_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl,
+                long nu, long nv, double u_scl, double v_scl, double *xos,
+                double *xsd, int job);
 /* plugin/trtt_3D_projectors_cubic.c:506-778 */
 int orc_PB3D_cubic(double *out, double *in, long nx, long ny, long nz,
                    double s_scl, int s_deg, long nu, long nv, double u_scl,

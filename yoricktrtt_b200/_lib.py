@@ -35,6 +35,8 @@ SIGNATURES = {
     "trtt_PB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I]),
     "trtt_CB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _dp, _dp, _L, _D, _dp, _L, _L, _D, _D, _dp, _dp, _I]),
     "trtt_DD_PB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_DD_CB3D": (_I, [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _dp, _dp, _I]),
+    "trtt_b200_dd_cb3d": (_I, [_dp, _dp, _L, _L, _L, _D, _L, _L, _D, _D, _L, _dp, _dp, _I]),
     "trtt_PB3D_cubic": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I]),
     "trtt_CB3D_cubic": (_I, [_dp, _dp, _L, _L, _L, _D, _I, _L, _L, _D, _D, _dp, _dp, _I]),
     "lf2d_direct": (None, [_vp, _D, _D, _dp, _dp, _I]),

@@ -461,6 +461,101 @@ int trtt_DD_PB3D(double *out, double *in, long nx, long ny, long nz, double s_sc
   return 0;
 }
 
+// ---- distance-driven 3D cone beam ---------------------------------------
+// The reference's unfinished trtt_DD_CB3D (plugin/trtt_3D_projectors.c:
+// 1340-1434, commented out there) completed as in the oracle; per-view
+// coefficients in the reference's operand order.
+static ParamsDDC ddc_view(long nx, long ny, long nz, double s_scl, long nu, long nv, double u_scl,
+                          double v_scl, const double *xos, const double *xsd)
+{
+  const double a1 = xsd[0], a2 = xsd[1], a3 = xsd[2], a4 = xsd[3];
+  const double a5 = xsd[4], a6 = xsd[5], a7 = xsd[6], a8 = xsd[7];
+  const double a9 = xsd[8], a10 = xsd[9], a11 = xsd[10], a12 = xsd[11];
+  const double o1 = xos[0], o2 = xos[1], o3 = xos[2], o4 = xos[3];
+  const double o5 = xos[4], o6 = xos[5], o7 = xos[6], o8 = xos[7];
+  const double o9 = xos[8], o10 = xos[9], o11 = xos[10], o12 = xos[11];
+  const double a1inv = -1.0 * (1.0 / a1);
+  const double b1 = a6 + a1inv * a5 * a2, c1 = a10 + a1inv * a9 * a2;
+  const double b2 = a7 + a1inv * a5 * a3, c2 = a11 + a1inv * a9 * a3;
+  const double b3 = a8 + a1inv * a5 * a4, c3 = a12 + a1inv * a9 * a4;
+  ParamsDDC P;
+  std::memset(&P, 0, sizeof(P));
+  P.nx = (int)nx; P.ny = (int)ny; P.nz = (int)nz; P.nu = (int)nu; P.nv = (int)nv;
+  P.u_scl = u_scl;
+  P.v_scl = v_scl;
+  P.s3 = s_scl * s_scl * s_scl;
+  P.o1 = o1; P.o2 = o2; P.o3 = o3; P.o4 = o4;
+  P.nv_x = b1 * o5 + b2 * o9;  P.nu_x = c1 * o5 + c2 * o9;
+  P.nv_y = b1 * o6 + b2 * o10; P.nu_y = c1 * o6 + c2 * o10;
+  P.nv_z = b1 * o7 + b2 * o11; P.nu_z = c1 * o7 + c2 * o11;
+  P.nv_c = b1 * o8 + b2 * o12; P.nu_c = c1 * o8 + c2 * o12;
+  P.d_x = a1 * o1 + a2 * o5 + a3 * o9;
+  P.d_y = a1 * o2 + a2 * o6 + a3 * o10;
+  P.d_z = a1 * o3 + a2 * o7 + a3 * o11;
+  P.d_c = a1 * o4 + a2 * o8 + a3 * o12;
+  P.a4sqr = a4 * a4;
+  P.a4m = -1.0 * a4;
+  P.a8 = a8;
+  P.a12 = a12;
+  P.b3 = b3;
+  P.c3 = c3;
+  P.axis = (std::fabs(P.nv_y) > std::fabs(P.nv_x)) ? 2 : 1;
+  return P;
+}
+
+int trtt_b200_dd_cb3d(double *out, const double *in, long nx, long ny, long nz, double s_scl,
+                      long nu, long nv, double u_scl, double v_scl, long nviews, const double *xos,
+                      const double *xsd, int job)
+{
+  clear_error();
+  if (!out || !in || !xos || !xsd) return fail("dd_cb3d: null argument");
+  if (!dim_ok(nx) || !dim_ok(ny) || !dim_ok(nz) || !dim_ok(nu) || !dim_ok(nv) || nviews < 1 ||
+      nviews > 65535)
+    return fail("dd_cb3d: dimensions out of range (views in [1, 65535])");
+  std::vector<ParamsDDC> hv(nviews);
+  for (long v = 0; v < nviews; ++v)
+    hv[v] = ddc_view(nx, ny, nz, s_scl, nu, nv, u_scl, v_scl, xos + 12 * v, xsd + 12 * v);
+  DropIn &D = dropin();
+  std::lock_guard<std::mutex> lock(D.mu);
+  TRTT_CK(D.init());
+  TRTT_CK(cudaSetDevice(D.device));
+  cudaStream_t st = D.stream;
+  const long nvox = nx * ny * nz, ndet = nu * nv * nviews;
+  const long nin = job == 0 ? nvox : ndet, nout = job == 0 ? ndet : nvox;
+  TRTT_CK(D.geom.ensure(sizeof(ParamsDDC) * nviews));
+  TRTT_CK(cudaMemcpyAsync(D.geom.p, hv.data(), sizeof(ParamsDDC) * nviews, cudaMemcpyHostToDevice, st));
+  TRTT_CK(D.err.ensure(sizeof(int)));
+  TRTT_CK(cudaMemsetAsync(D.err.p, 0, sizeof(int), st));
+  TRTT_CK(D.in64.ensure(sizeof(double) * nin));
+  TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+  TRTT_CK(D.out64.ensure(sizeof(double) * nout));
+  TRTT_CK(cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, st));
+  const ParamsDDC *vd = static_cast<const ParamsDDC *>(D.geom.p);
+  if (job == 0)
+    TRTT_CK(launch_ddc_fwd(vd, (int)nviews, nvox, D.in64.as<double>(), D.out64.as<double>(), nu * nv,
+                           D.err.as<int>(), st));
+  else
+    TRTT_CK(launch_ddc_back(vd, (int)nviews, nvox, D.in64.as<double>(), nu * nv, D.out64.as<double>(),
+                            D.err.as<int>(), st));
+  count_launch();
+  int herr = 0;
+  TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TRTT_CK(cudaStreamSynchronize(st));
+  if (herr) {
+    std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
+    return fail("dd_cb3d: a voxel lies in the source plane (wk == 0)");
+  }
+  TRTT_CK(cudaMemcpyAsync(out, D.out64.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
+  TRTT_CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int trtt_DD_CB3D(double *out, double *in, long nx, long ny, long nz, double s_scl, long nu,
+                 long nv, double u_scl, double v_scl, double *xos, double *xsd, int job)
+{
+  return trtt_b200_dd_cb3d(out, in, nx, ny, nz, s_scl, nu, nv, u_scl, v_scl, 1, xos, xsd, job);
+}
+
 // ---- 1-based COO product ------------------------------------------------
 int trtt_mvmult(double *out, double *in, long number, double *a, long *i, long *j)
 {

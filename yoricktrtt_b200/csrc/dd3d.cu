@@ -123,6 +123,163 @@ cudaError_t launch_dd_back(const ParamsDD &P, const double *det, double *vol, cu
 }
 
 // ---------------------------------------------------------------------------
+// Distance-driven 3D cone beam: the reference's unfinished trtt_DD_CB3D
+// (plugin/trtt_3D_projectors.c:1340-1434) completed as in the oracle: the
+// section of the voxel perpendicular to x (or y) is projected from the
+// source through its four corners, the footprint is their bounding detector
+// rectangle (clamped like trtt_DD_PB3D), and the weight spreads the voxel's
+// cone-beam detector integral s^3 magn^2 delta_u delta_v uniformly over the
+// unclamped rectangle.  FP64 throughout, reference operand order; the
+// direct projector scatters with FP64 atomics (one view per grid row), the
+// transpose gathers per voxel with the same weights (exact adjoint).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dd_axis_b(double b1, double b2, int n, double scl, DDAxis &a)
+{
+  const double last = (double)(n - 1);
+  b1 = b1 >= 0 ? b1 : 0;
+  b1 = b1 <= last ? b1 : last;
+  b2 = b2 >= 0 ? b2 : 0;
+  b2 = b2 <= last ? b2 : last;
+  a.b1 = b1;
+  a.b2 = b2;
+  a.up = ceil(b1);
+  a.down = floor(b2);
+  a.left = floor(b1);
+  a.scl = scl;
+  a.nint = (long)dsub(a.down, a.up);
+  a.neff = (long)dsub(ceil(b2), a.left);
+}
+
+// Footprint of voxel (i, j, k) in one view; false when it contributes nothing.
+__device__ __forceinline__ bool dd_cone_voxel(const ParamsDDC &P, int i, int j, int k, DDAxis &au,
+                                              DDAxis &av, double &h_norm, long &base, int *err)
+{
+  const double x = i, y = j, z = k;
+  const double wk = dadd(dadd(dadd(dmul(P.o1, x), dmul(P.o2, y)), dmul(P.o3, z)), P.o4);
+  if (wk == 0.0) {
+    atomicOr(err, 1);
+    return false;
+  }
+  double ub1 = 0, ub2 = 0, vb1 = 0, vb2 = 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double hs = (c & 1) ? 0.5 : -0.5, hz = (c & 2) ? 0.5 : -0.5;
+    const double cx = dadd(x, P.axis == 1 ? hs : 0.0), cy = dadd(y, P.axis == 2 ? hs : 0.0);
+    const double cz = dadd(z, hz);
+    const double nu_ = dadd(dadd(dadd(dmul(P.nu_x, cx), dmul(P.nu_y, cy)), dmul(P.nu_z, cz)), P.nu_c);
+    const double nv_ = dadd(dadd(dadd(dmul(P.nv_x, cx), dmul(P.nv_y, cy)), dmul(P.nv_z, cz)), P.nv_c);
+    const double de = dadd(dadd(dadd(dmul(P.d_x, cx), dmul(P.d_y, cy)), dmul(P.d_z, cz)), P.d_c);
+    const double qc = ddiv(P.a4m, de);
+    const double uc = dadd(dmul(qc, nu_), P.c3), vc = dadd(dmul(qc, nv_), P.b3);
+    if (!(isfinite(uc) && isfinite(vc))) return false;
+    if (c == 0) {
+      ub1 = ub2 = uc;
+      vb1 = vb2 = vc;
+    } else {
+      ub1 = uc < ub1 ? uc : ub1;
+      ub2 = uc > ub2 ? uc : ub2;
+      vb1 = vc < vb1 ? vc : vb1;
+      vb2 = vc > vb2 ? vc : vb2;
+    }
+  }
+  const double Du = dsub(ub2, ub1), Dv = dsub(vb2, vb1);
+  const double num_u = dadd(dadd(dadd(dmul(P.nu_x, x), dmul(P.nu_y, y)), dmul(P.nu_z, z)), P.nu_c);
+  const double num_v = dadd(dadd(dadd(dmul(P.nv_x, x), dmul(P.nv_y, y)), dmul(P.nv_z, z)), P.nv_c);
+  const double den = dadd(dadd(dadd(dmul(P.d_x, x), dmul(P.d_y, y)), dmul(P.d_z, z)), P.d_c);
+  const double q = ddiv(P.a4m, den);
+  const double uc = dadd(dmul(q, num_u), P.c3), vc = dadd(dmul(q, num_v), P.b3);
+  const double magn = ddiv(P.a4m, wk);
+  const double va = dmul(dsub(vc, P.a8), P.v_scl);
+  const double vca8sqr = dmul(va, va);
+  const double dv = dsqrt(dadd(1.0, ddiv(vca8sqr, P.a4sqr)));
+  const double ua = dmul(dsub(uc, P.a12), P.u_scl);
+  const double du = dsqrt(dadd(1.0, ddiv(dmul(ua, ua), dadd(P.a4sqr, vca8sqr))));
+  h_norm = ddiv(dmul(dmul(dmul(P.s3, dmul(magn, magn)), du), dv),
+                dmul(dmul(dmul(P.u_scl, P.v_scl), Du), Dv));
+  if (!isfinite(h_norm)) return false;
+  dd_axis_b(ub1, ub2, P.nu, P.u_scl, au);
+  dd_axis_b(vb1, vb2, P.nv, P.v_scl, av);
+  if (!(au.neff > 0 && av.neff > 0)) return false;
+  base = (long)av.left * P.nu + (long)au.left;
+  return true;
+}
+
+__global__ void k_ddc_fwd(const ParamsDDC *__restrict__ views, const double *__restrict__ vol,
+                          double *__restrict__ det, long det_stride, int *err)
+{
+  const ParamsDDC &P = views[blockIdx.y];
+  const long n = (long)P.nx * P.ny * P.nz;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const double x = vol[idx];
+  const int i = (int)(idx % P.nx);
+  const long r = idx / P.nx;
+  const int j = (int)(r % P.ny), k = (int)(r / P.ny);
+  if (x == 0.0) {
+    // no contribution, but the source-plane failure applies to every voxel
+    const double wk = dadd(dadd(dadd(dmul(P.o1, (double)i), dmul(P.o2, (double)j)),
+                                dmul(P.o3, (double)k)), P.o4);
+    if (wk == 0.0) atomicOr(err, 1);
+    return;
+  }
+  DDAxis au, av;
+  double h;
+  long base;
+  if (!dd_cone_voxel(P, i, j, k, au, av, h, base, err)) return;
+  double *d = det + (long)blockIdx.y * det_stride;
+  for (long m = 0; m < av.neff; ++m) {
+    const double hv = dmul(h, dd_cell(av, m, false));
+    for (long l = 0; l < au.neff; ++l)
+      atomicAdd(d + base + m * P.nu + l, dmul(dmul(hv, dd_cell(au, l, false)), x));
+  }
+}
+
+__global__ void k_ddc_back(const ParamsDDC *__restrict__ views, int nviews,
+                           const double *__restrict__ det, long det_stride,
+                           double *__restrict__ vol, int *err)
+{
+  const ParamsDDC &P0 = views[0];
+  const long n = (long)P0.nx * P0.ny * P0.nz;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int i = (int)(idx % P0.nx);
+  const long r = idx / P0.nx;
+  const int j = (int)(r % P0.ny), k = (int)(r / P0.ny);
+  double acc = vol[idx];
+  for (int v = 0; v < nviews; ++v) {
+    DDAxis au, av;
+    double h;
+    long base;
+    if (!dd_cone_voxel(views[v], i, j, k, au, av, h, base, err)) continue;
+    const double *d = det + (long)v * det_stride;
+    for (long m = 0; m < av.neff; ++m) {
+      const double hv = dmul(h, dd_cell(av, m, false));
+      for (long l = 0; l < au.neff; ++l)
+        acc = dadd(acc, dmul(dmul(hv, dd_cell(au, l, false)), d[base + m * P0.nu + l]));
+    }
+  }
+  vol[idx] = acc;
+}
+
+cudaError_t launch_ddc_fwd(const ParamsDDC *views_dev, int nviews, long nvox, const double *vol,
+                           double *det, long det_stride, int *err, cudaStream_t st)
+{
+  if (nviews <= 0 || nvox <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((nvox + 255) / 256), (unsigned)nviews);
+  k_ddc_fwd<<<grid, 256, 0, st>>>(views_dev, vol, det, det_stride, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ddc_back(const ParamsDDC *views_dev, int nviews, long nvox, const double *det,
+                            long det_stride, double *vol, int *err, cudaStream_t st)
+{
+  if (nviews <= 0 || nvox <= 0) return cudaSuccess;
+  k_ddc_back<<<(unsigned)((nvox + 255) / 256), 256, 0, st>>>(views_dev, nviews, det, det_stride, vol,
+                                                            err);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // 1-based COO product: out[i[k]-1] += a[k] * in[j[k]-1]
 // ---------------------------------------------------------------------------
 __global__ void k_mvmult(const double *__restrict__ a, const long *__restrict__ i,

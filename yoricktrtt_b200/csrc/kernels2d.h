@@ -63,6 +63,23 @@ struct ParamsDD {
   double Du, Dv, h_norm;
 };
 cudaError_t launch_dd_fwd(const ParamsDD &P, const double *vol, double *det, cudaStream_t st);
+
+// Cone-beam distance-driven view (dd3d.cu): the coefficients of trtt_CB3D
+// (num_u, num_v, den, wk) and the voxel-section direction (1: x, 2: y).
+struct ParamsDDC {
+  int nx, ny, nz, nu, nv, axis;
+  double u_scl, v_scl, s3;
+  double o1, o2, o3, o4;
+  double nu_x, nu_y, nu_z, nu_c, nv_x, nv_y, nv_z, nv_c;
+  double d_x, d_y, d_z, d_c;
+  double a4m, a4sqr, a8, a12, b3, c3;
+};
+// views_dev: nviews device records; det: nviews images of det_stride
+// doubles; err |= 1 when a voxel centre lies in the source plane.
+cudaError_t launch_ddc_fwd(const ParamsDDC *views_dev, int nviews, long nvox, const double *vol,
+                           double *det, long det_stride, int *err, cudaStream_t st);
+cudaError_t launch_ddc_back(const ParamsDDC *views_dev, int nviews, long nvox, const double *det,
+                            long det_stride, double *vol, int *err, cudaStream_t st);
 cudaError_t launch_dd_back(const ParamsDD &P, const double *det, double *vol, cudaStream_t st);
 
 // Sparse COO product out[i-1] += a * in[j-1] (spmv.cu).

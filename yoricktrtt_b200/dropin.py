@@ -110,6 +110,24 @@ def dd_pb3d(out, vol, scan, view, job):
     _lib.check(rc, "trtt_DD_PB3D")
 
 
+def dd_cb3d(out, vol, scan, view, job):
+    """trtt_DD_CB3D on one view (host FP64 arrays, accumulate into out)."""
+    lib = _lib.load()
+    rc = lib.trtt_DD_CB3D(dptr(out), dptr(vol), scan.nx, scan.ny, scan.nz, scan.s_scl,
+                          scan.nu, scan.nv, scan.u_scl, scan.v_scl, dptr(_c12(scan.xos[view])),
+                          dptr(_c12(scan.xsd[view])), job)
+    _lib.check(rc, "trtt_DD_CB3D")
+
+
+def dd_cb3d_batch(out, x, scan, job):
+    """trtt_b200_dd_cb3d over all views of `scan`."""
+    lib = _lib.load()
+    rc = lib.trtt_b200_dd_cb3d(dptr(out), dptr(x), scan.nx, scan.ny, scan.nz, scan.s_scl,
+                               scan.nu, scan.nv, scan.u_scl, scan.v_scl, scan.nviews,
+                               dptr(np.ascontiguousarray(scan.xos)),
+                               dptr(np.ascontiguousarray(scan.xsd)), job)
+    _lib.check(rc, "trtt_b200_dd_cb3d")
+
 def p2d(name: str, out, img, scan, view, job, table=None):
     """trtt_PB2D / trtt_FB2D (table) or _cubic, one view of a Scan2D."""
     lib = _lib.load()
