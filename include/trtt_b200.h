@@ -231,6 +231,32 @@ int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *plan, int band_rows, int warps)
  * pair kernel's shared memory (band + 2 profiles per warp) does not fit. */
 int trtt_b200_plan3d_set_columns(trtt_b200_plan3d *plan, int cols);
 
+/* Weighted least-squares data term in one persistent launch.  No single
+ * counterpart in the reference: it is the cost evaluation of its 4D
+ * reconstruction (Tomography_4D/Ytrtt4D_optim.i:87-223) with the per-gate
+ * projection of Ytrtt_3D_projectors.i:254-375.  For the plan's views (gates
+ * set by plan3d_set_gates, else one volume):
+ *   resid = W (H x - y), *cost = 1/2 sum W (H x - y)^2 (FP64, written),
+ *   grad += H^T resid (per gate).
+ * vol and grad: device, column layout (TRTT_B200_LAYOUT_COLUMNS), gates
+ * stacked; y and w: device [view][nv][nu] (w NULL: unit weights); cost:
+ * device, one double.  Closed-form model, column-factorised views (else
+ * -1).  One cooperative launch of resident CTAs draws (view, band) items,
+ * then (gate, column block) items from a device queue; a column item waits,
+ * bounded by the plan's wait limit, for every band item; a wait that runs
+ * out makes the next plan3d_status call fail ("bounded device wait ran
+ * out") and the launch returns early.
+ * Not synchronous: the results are ready when `stream` is. */
+int trtt_b200_plan3d_wls_grad(trtt_b200_plan3d *plan, const float *vol, const float *y,
+                              const float *w, float *grad, double *cost, void *stream);
+/* Shape of the persistent launch: detector-row band height (0 keeps; 32 by
+ * default), CTAs per SM (1: up to 128 registers per thread, 2: 64; 0
+ * keeps), the bound of the device wait in seconds (0 keeps; 2 s by
+ * default) and extra_wait, a test hook: column items also wait for
+ * extra_wait band items that do not exist, so the bounded wait runs out. */
+int trtt_b200_plan3d_set_persistent(trtt_b200_plan3d *plan, int band_rows, int ctas_per_sm,
+                                    double wait_seconds, int extra_wait);
+
 /* 1 if every view of the plan uses the column-factorised kernels. */
 int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
 

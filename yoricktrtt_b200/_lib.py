@@ -58,6 +58,8 @@ SIGNATURES = {
     "trtt_b200_plan3d_factorized": (_I, [_vp]),
     "trtt_b200_plan3d_set_columns": (_I, [_vp, _I]),
     "trtt_b200_plan3d_groups": (_I, [_vp, _vp]),
+    "trtt_b200_plan3d_wls_grad": (_I, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "trtt_b200_plan3d_set_persistent": (_I, [_vp, _I, _I, _D, _I]),
     "trtt_b200_plan3d_set_symmetry": (_I, [_vp, _I]),
     "trtt_b200_plan3d_set_group_tiles": (_I, [_vp, _I, _I, _I, _L]),
     "trtt_b200_plan3d_destroy": (_I, [_vp]),

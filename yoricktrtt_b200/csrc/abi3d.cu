@@ -43,6 +43,10 @@ struct trtt_b200_plan3d {
   DevBuf groups[3];
   int gband[3] = {64, 32, 32};  // direct: band rows per group size
   long back_chunk_bytes = 32L << 20;  // transpose: detector bytes per launch
+  // persistent weighted least-squares launch
+  int wls_rows = 32, wls_ctas = 1, wls_extra = 0;
+  long long wls_wait_ns = 2000000000LL;
+  DevBuf resid, wls_parts, wls_queue;
 };
 
 static int group_size_of(int idx) { return idx == 2 ? 4 : idx + 1; }
@@ -276,6 +280,74 @@ extern "C" int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *pl, int band_r
   return 0;
 }
 
+extern "C" int trtt_b200_plan3d_set_persistent(trtt_b200_plan3d *pl, int band_rows, int ctas_per_sm,
+                                               double wait_seconds, int extra_wait)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_persistent: null plan");
+  if (band_rows < 0 || (band_rows > 0 && band_rows < 2))
+    return fail("plan3d_set_persistent: band rows must be 0 (keep) or >= 2");
+  if (ctas_per_sm < 0 || ctas_per_sm > 2) return fail("plan3d_set_persistent: CTAs per SM must be 0, 1 or 2");
+  if (!(wait_seconds >= 0.0) || wait_seconds > 60.0)
+    return fail("plan3d_set_persistent: wait limit must be in [0, 60] s (0 keeps)");
+  if (extra_wait < 0) return fail("plan3d_set_persistent: negative extra wait");
+  if (band_rows) {
+    const int r = std::min(band_rows, pl->P.nv);
+    if (wls_smem(pl->P.nu, r) > 227u * 1024u) return fail("plan3d_set_persistent: band does not fit in shared memory");
+    pl->wls_rows = band_rows;
+  }
+  if (ctas_per_sm) pl->wls_ctas = ctas_per_sm;
+  if (wait_seconds > 0.0) pl->wls_wait_ns = (long long)(wait_seconds * 1e9);
+  pl->wls_extra = extra_wait;
+  return 0;
+}
+
+extern "C" int trtt_b200_plan3d_wls_grad(trtt_b200_plan3d *pl, const float *vol, const float *y,
+                                         const float *w, float *grad, double *cost, void *stream)
+{
+  clear_error();
+  if (!pl || !vol || !y || !grad || !cost) return fail("plan3d_wls_grad: null argument");
+  if (!pl->factorized || pl->P.model != MODEL_CUBIC)
+    return fail("plan3d_wls_grad: needs the closed-form model and column-factorised views");
+  cudaStream_t st = (cudaStream_t)stream;
+  const Params3D &P = pl->P;
+  int dev = 0, sms = 0, coop = 0;
+  TRTT_CK(cudaGetDevice(&dev));
+  TRTT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  TRTT_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return fail("plan3d_wls_grad: the device has no cooperative launch");
+  WlsLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.P = P;
+  L.views = pl->views.as<View3D>();
+  L.nviews = (int)pl->nviews;
+  L.gate_ptr = pl->gate_ptr.as<int>();
+  L.entries = pl->entries.as<GateEntry>();
+  L.ngates = pl->nt;
+  L.vol = vol;
+  L.gate_stride = (long)P.nx * P.ny * P.nz;
+  L.y = y;
+  L.w = w;
+  L.grad = grad;
+  L.cost = cost;
+  L.band_rows = std::min(pl->wls_rows, P.nv);
+  L.ctas_per_sm = pl->wls_ctas;
+  L.extra_wait = pl->wls_extra;
+  L.wait_ns = pl->wls_wait_ns;
+  L.err = pl->err.as<int>();
+  const long nbands = (P.nv + L.band_rows - 1) / L.band_rows;
+  TRTT_CK(pl->resid.ensure(sizeof(float) * (size_t)pl->nviews * P.nu * P.nv));
+  TRTT_CK(pl->wls_parts.ensure(sizeof(double) * (size_t)(pl->nviews * nbands)));
+  TRTT_CK(pl->wls_queue.ensure(sizeof(unsigned) * 2));
+  TRTT_CK(cudaMemsetAsync(pl->wls_queue.p, 0, sizeof(unsigned) * 2, st));
+  L.resid = pl->resid.as<float>();
+  L.cost_parts = pl->wls_parts.as<double>();
+  L.queue = pl->wls_queue.as<unsigned>();
+  TRTT_CK(launch_wls_persistent(L, sms, st));
+  count_launch();
+  return 0;
+}
+
 extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
 {
   return pl && pl->factorized ? 1 : 0;
@@ -432,6 +504,7 @@ extern "C" int trtt_b200_plan3d_status(trtt_b200_plan3d *pl, void *stream)
   TRTT_CK(cudaMemcpy(&h, pl->err.p, sizeof(int), cudaMemcpyDeviceToHost));
   TRTT_CK(cudaMemset(pl->err.p, 0, sizeof(int)));
   if (h & TRTT_ERR_SOURCE_PLANE) return fail("a voxel lies in the source plane (wk == 0)");
+  if (h & TRTT_ERR_STALL) return fail("a bounded device wait ran out (persistent launch stalled)");
   if (h) return fail("device error flag set");
   return 0;
 }
@@ -444,6 +517,9 @@ extern "C" int trtt_b200_plan3d_destroy(trtt_b200_plan3d *pl)
   pl->gate_ptr.release();
   pl->entries.release();
   for (auto &gb : pl->groups) gb.release();
+  pl->resid.release();
+  pl->wls_parts.release();
+  pl->wls_queue.release();
   pl->scratch.release();
   pl->err.release();
   delete pl;

@@ -85,6 +85,36 @@ struct GroupBackLaunch {
   int *err;
 };
 
+// Weighted least-squares data term of a scan in one persistent cooperative
+// launch (persist4d.cu; closed-form model, column-factorised views, gates):
+// resid = W (H x - y), *cost = 1/2 sum W (H x - y)^2, grad += H^T resid.
+struct WlsLaunch {
+  Params3D P;
+  const View3D *views;
+  int nviews;
+  const int *gate_ptr;       // ngates+1 offsets into entries
+  const GateEntry *entries;
+  int ngates;
+  const float *vol;          // column layout, gates stacked
+  long gate_stride;
+  const float *y, *w;        // [view][nv][nu]; w may be null (unit weights)
+  float *resid;              // [view][nv][nu] scratch
+  float *grad;               // column layout, gates stacked, accumulated
+  double *cost_parts;        // one per band item
+  double *cost;              // device, written
+  unsigned *queue;           // [0] next item, [1] finished band items; zero before launch
+  int band_rows;
+  int ctas_per_sm;           // 1 or 2 (0: 1): register budget of 128 or 64 per thread
+  int extra_wait;            // column items also wait for this many band items (test hook)
+  long long wait_ns;         // bound of that wait
+  int *err;
+  // filled by launch_wls_persistent
+  int nbands, kchunks, n_band_items, n_col_items;
+};
+size_t wls_smem(int nu, int band_rows);
+int wls_kp(int nz);
+cudaError_t launch_wls_persistent(WlsLaunch L, int sms, cudaStream_t st);
+
 size_t group_fwd_smem(int G, int band_rows, int utile, int warps);
 int group_orbits(int G, int nx, int ny);
 cudaError_t launch_fwd3d_group(const GroupFwdLaunch &L, int G, cudaStream_t st);

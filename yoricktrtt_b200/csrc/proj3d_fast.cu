@@ -11,12 +11,10 @@
 
 #include <climits>
 
-#include "fast3d.cuh"
+#include "fast3d_items.cuh"
 #include "kernels.h"
 
 namespace trtt {
-
-static constexpr int SPREAD_CHUNKS = 16;  // footprints up to 512 cells wide spread from registers
 
 // ---------------------------------------------------------------------------
 // Direct projector
@@ -32,7 +30,7 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   __shared__ int s_next;
   const int nwarps = blockDim.x >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nu = P.nu, nv = P.nv, nz = P.nz;
+  const int nu = P.nu, nv = P.nv;
   float *acc = sm;
   float *prof = sm + band_rows * nu + warp * nu;
   float *wv = sm + band_rows * nu + nwarps * nu + warp * band_rows;
@@ -46,102 +44,7 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   for (int t = threadIdx.x; t < band_rows * nu; t += blockDim.x) acc[t] = 0.f;
   for (int t = lane; t < nu; t += 32) prof[t] = 0.f;
   __syncthreads();
-  const View3D &V = sV;
-  const int ncols = P.nx * P.ny;
-  const int nchunks = (ncols + 31) >> 5;
-
-  for (;;) {
-    int chunk = 0;
-    if (lane == 0) chunk = atomicAdd(&s_next, 1);
-    chunk = __shfl_sync(FULLM, chunk, 0);
-    if (chunk >= nchunks) break;
-    const int mycol = (chunk << 5) + lane;
-    ColGeo<MODEL_CUBIC> c;
-    bool hit = false;
-    if (mycol < ncols) {
-      column_geo<GEOM, MODEL_CUBIC>(P, V, mycol % P.nx, mycol / P.nx, 0, c);
-      if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
-      hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
-    }
-    unsigned mask = __ballot_sync(FULLM, hit);
-    while (mask) {
-      const int src = __ffs(mask) - 1;
-      mask &= mask - 1;
-      const ColGeo<MODEL_CUBIC> cc = shfl_colc(c, src);
-      const int col = (chunk << 5) + src;
-      const int vl = cc.vax.lo, vr = cc.vax.lo + cc.vax.n;
-      const int rb = max(vl, v0), re = min(vr, v1), nr = re - rb;
-      for (int r = lane; r < nr; r += 32) wv[r] = axis_weight<MODEL_CUBIC>(cc.vax, rb - vl + r, P);
-      int lo = INT_MAX, hi = INT_MIN;
-      const long cbase = (long)col * nz;
-      for (int k0 = lane; k0 < nz; k0 += 64) {
-        const int k1 = k0 + 32;
-        const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
-        const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
-        if (x0 == 0.0f && x1 == 0.0f) continue;
-        UPair up;
-        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
-        if (x0 == 0.0f) up.n0 = 0;
-        if (x1 == 0.0f) up.n1 = 0;
-        const int L = max(up.n0, up.n1);
-        if (L <= 0) continue;
-        const float2 xr = mul2(make_float2(x0, x1), up.rho);
-        float2 Fp = first_edge_prim2(up);
-        float2 lf = f2(1.0f);
-        for (int l = 0; l < L; ++l) {
-          const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
-          const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
-          if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
-          if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
-          Fp = F;
-          lf = add2(lf, f2(1.0f));
-        }
-        if (up.n0 > 0) {
-          lo = min(lo, up.lo0);
-          hi = max(hi, up.lo0 + up.n0);
-        }
-        if (up.n1 > 0) {
-          lo = min(lo, up.lo1);
-          hi = max(hi, up.lo1 + up.n1);
-        }
-      }
-      lo = __reduce_min_sync(FULLM, lo);
-      hi = __reduce_max_sync(FULLM, hi);
-      __syncwarp();
-      if (lo < hi && hi - lo <= 32 * SPREAD_CHUNKS) {
-        // profile read once into registers (and cleared), then one shared
-        // atomic per (row, cell) of the footprint
-        float pv[SPREAD_CHUNKS];
-#pragma unroll
-        for (int c = 0; c < SPREAD_CHUNKS; ++c) {
-          const int u = lo + lane + 32 * c;
-          pv[c] = 0.f;
-          if (u < hi) {
-            pv[c] = prof[u];
-            prof[u] = 0.f;
-          }
-        }
-        for (int r = 0; r < nr; ++r) {
-          const float w = wv[r];
-          float *row = acc + (rb - v0 + r) * nu;
-#pragma unroll
-          for (int c = 0; c < SPREAD_CHUNKS; ++c) {
-            const int u = lo + lane + 32 * c;
-            if (u < hi) atomicAdd(row + u, w * pv[c]);
-          }
-        }
-      } else if (lo < hi) {
-        for (int r = 0; r < nr; ++r) {
-          const float w = wv[r];
-          float *row = acc + (rb - v0 + r) * nu;
-          for (int u = lo + lane; u < hi; u += 32) atomicAdd(row + u, w * prof[u]);
-        }
-        __syncwarp();
-        for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;
-      }
-      __syncwarp();
-    }
-  }
+  band_item<GEOM>(P, sV, vol, gate_stride, v0, v1, band_rows, acc, prof, wv, &s_next, err);
   __syncthreads();
   float *out = sino + (long)vi * sino_view_stride;
   const int nrow = v1 - v0;
@@ -441,130 +344,14 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
 {
   extern __shared__ float sm[];
   const int nwarps = blockDim.x >> 5;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nu = P.nu, nz = P.nz;
+  const int warp = threadIdx.x >> 5;
   const int ncols = P.nx * P.ny;
   const int col = blockIdx.x * nwarps + warp;
   if (col >= ncols) return;
-  float *Q = sm + warp * nu;
-  const int i = col % P.nx, j = col / P.nx;
-  const int kbase = blockIdx.y * (64 * KP);
   const int gate = blockIdx.z;
-  const int e0 = gate_ptr[gate], e1 = gate_ptr[gate + 1];
-  float2 acc[KP], cmp[KP];
-#pragma unroll
-  for (int p = 0; p < KP; ++p) {
-    acc[p] = f2(0.f);
-    cmp[p] = f2(0.f);
-  }
-
-  for (int eb = e0; eb < e1; eb += 32) {
-    const int me = eb + lane;
-    ColGeo<MODEL_CUBIC> mine;
-    int myview = 0;
-    float myw = 0.f;
-    const GateEntry ge = (me < e1) ? entries[me] : GateEntry{-1, 0.f};
-    if (ge.view >= view_lo && ge.view < view_hi) {
-      myview = ge.view;
-      myw = ge.w;
-      column_geo<GEOM, MODEL_CUBIC>(P, views[myview], i, j, 0, mine);
-      if (mine.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
-    } else {
-      mine.vax.n = 0;
-      mine.bad = 1;
-    }
-    const int cnt = min(32, e1 - eb);
-    for (int s = 0; s < cnt; ++s) {
-      const int nvx = __shfl_sync(FULLM, mine.vax.n, s);
-      const int bd = __shfl_sync(FULLM, mine.bad, s);
-      if (bd || nvx <= 0) continue;
-      const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
-      const int view = __shfl_sync(FULLM, myview, s);
-      const float wgt = __shfl_sync(FULLM, myw, s);
-      const View3D &V = views[view];
-      UPair up[KP];
-      int lo = INT_MAX, hi = INT_MIN;
-#pragma unroll
-      for (int p = 0; p < KP; ++p) {
-        const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
-        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up[p]);
-        if (k0 >= nz) up[p].n0 = 0;
-        if (k1 >= nz) up[p].n1 = 0;
-        if (up[p].n0 > 0) {
-          lo = min(lo, up[p].lo0);
-          hi = max(hi, up[p].lo0 + up[p].n0);
-        }
-        if (up[p].n1 > 0) {
-          lo = min(lo, up[p].lo1);
-          hi = max(hi, up[p].lo1 + up[p].n1);
-        }
-      }
-      lo = __reduce_min_sync(FULLM, lo);
-      hi = __reduce_max_sync(FULLM, hi);
-      if (lo >= hi) continue;
-      // v-collapsed profile Q[u] = sum_v wv(v) pix[v][u], u in [lo, hi).
-      // Each lane keeps up to QC cells of Q in registers (u = lo + lane + 32c)
-      // and walks the footprint rows; the QC loads of a row are independent,
-      // so a warp keeps many loads in flight.
-      const int npv = cc.vax.n;
-      const float *img0 = sino + (long)(view - view_lo) * sino_view_stride;
-      constexpr int QC = 16;
-      for (int ub = lo; ub < hi; ub += 32 * QC) {
-        float q[QC];
-#pragma unroll
-        for (int c = 0; c < QC; ++c) q[c] = 0.f;
-        for (int m0 = 0; m0 < npv; m0 += 32) {
-          const int mn = min(32, npv - m0);
-          const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
-          for (int m = 0; m < mn; ++m) {
-            const float w = __shfl_sync(FULLM, wl, m);
-            const float *row = img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + lane;
-            float a[QC];
-#pragma unroll
-            for (int c = 0; c < QC; ++c) a[c] = (ub + lane + 32 * c < hi) ? __ldg(row + 32 * c) : 0.f;
-#pragma unroll
-            for (int c = 0; c < QC; ++c) q[c] = fmaf(w, a[c], q[c]);
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < QC; ++c)
-          if (ub + lane + 32 * c < hi) Q[ub + lane + 32 * c] = q[c];
-      }
-      __syncwarp();
-      // per-voxel gathers, two voxels per instruction
-#pragma unroll
-      for (int p = 0; p < KP; ++p) {
-        const int L = max(up[p].n0, up[p].n1);
-        if (L <= 0) continue;
-        float2 Fp = first_edge_prim2(up[p]);
-        float2 S = f2(0.f);
-        float2 lf = f2(1.0f);
-        for (int l = 0; l < L; ++l) {
-          const float2 F = cubic_prim2(fma2(lf, up[p].inc, up[p].start));
-          const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
-          const float q0 = (l < up[p].n0) ? Q[up[p].lo0 + l] : 0.0f;
-          const float q1 = (l < up[p].n1) ? Q[up[p].lo1 + l] : 0.0f;
-          S = fma2(w, make_float2(q0, q1), S);
-          Fp = F;
-          lf = add2(lf, f2(1.0f));
-        }
-        // Kahan (packed): acc += wgt * rho * S
-        const float2 term = mul2(mul2(up[p].rho, S), f2(wgt));
-        const float2 y = add2(term, make_float2(-cmp[p].x, -cmp[p].y));
-        const float2 t = add2(acc[p], y);
-        cmp[p] = add2(add2(t, make_float2(-acc[p].x, -acc[p].y)), make_float2(-y.x, -y.y));
-        acc[p] = t;
-      }
-      __syncwarp();
-    }
-  }
-  float *dst = vol + (long)gate * gate_stride + (long)col * nz;
-#pragma unroll
-  for (int p = 0; p < KP; ++p) {
-    const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
-    if (k0 < nz) dst[k0] += acc[p].x - cmp[p].x;
-    if (k1 < nz) dst[k1] += acc[p].y - cmp[p].y;
-  }
+  column_item<GEOM, KP, LoadNC>(P, views, entries, gate_ptr[gate], gate_ptr[gate + 1], view_lo,
+                                view_hi, sino, sino_view_stride, vol, gate_stride, col,
+                                blockIdx.y * (64 * KP), gate, sm + warp * P.nu, err);
 }
 
 // ---------------------------------------------------------------------------

@@ -115,6 +115,63 @@ class Projector3D:
             self._h, band_rows4, band_rows2, band_rows1, back_chunk_bytes),
             "trtt_b200_plan3d_set_group_tiles")
 
+    def wls_grad(self, vol, y, grad, w=None, cost=None):
+        """One persistent launch: grad += H^T W (H vol - y), returns the
+        device FP64 cost 1/2 sum W (H vol - y)^2 (columns layout, gates
+        stacked; y, w: (nviews, nv, nu) float32)."""
+        torch = _torch()
+        if cost is None:
+            cost = torch.zeros(1, dtype=torch.float64, device=vol.device)
+        self._check(vol, self.volume_shape("columns"), "vol")
+        self._check(grad, self.volume_shape("columns"), "grad")
+        self._check(y, self.detector_shape(), "y")
+        if w is not None:
+            self._check(w, self.detector_shape(), "w")
+        lib = _lib.load()
+        _lib.check(lib.trtt_b200_plan3d_wls_grad(
+            self._h, C.c_void_p(vol.data_ptr()), C.c_void_p(y.data_ptr()),
+            C.c_void_p(w.data_ptr()) if w is not None else None, C.c_void_p(grad.data_ptr()),
+            C.c_void_p(cost.data_ptr()), _stream_ptr(torch.cuda.current_stream())),
+            "trtt_b200_plan3d_wls_grad")
+        return cost
+
+    def set_persistent(self, band_rows=0, ctas_per_sm=0, wait_seconds=0.0, extra_wait=0):
+        _lib.check(_lib.load().trtt_b200_plan3d_set_persistent(
+            self._h, band_rows, ctas_per_sm, float(wait_seconds), extra_wait),
+            "trtt_b200_plan3d_set_persistent")
+
+    WLS_CANDIDATES = [(16, 1), (32, 1), (16, 2), (32, 2), (8, 2)]
+
+    def autotune_wls(self, vol, y, w=None, candidates=None, reps=2):
+        """Time the persistent launch with each (band rows, CTAs per SM)
+        candidate on the given data and keep the fastest; returns
+        ({candidate: ms}, choice)."""
+        torch = _torch()
+        grad = torch.zeros_like(vol)
+        times = {}
+        for cand in candidates or self.WLS_CANDIDATES:
+            try:
+                self.set_persistent(*cand)
+            except _lib.TrttError:
+                continue
+            self.wls_grad(vol, y, grad, w)
+            torch.cuda.synchronize()
+            best = math.inf
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                self.wls_grad(vol, y, grad, w)
+                b.record()
+                torch.cuda.synchronize()
+                best = min(best, a.elapsed_time(b))
+            times[cand] = best
+        self.status()
+        choice = min(times, key=times.get)
+        self.set_persistent(*choice)
+        self.wls_tiles = choice
+        return times, choice
+
     @property
     def factorized(self) -> bool:
         return bool(_lib.load().trtt_b200_plan3d_factorized(self._h))
