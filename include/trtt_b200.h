@@ -421,6 +421,25 @@ int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, fl
                       double frtol, double *f_hist, double *t_hist, trtt_b200_vmlmb_info *info,
                       void *stream);
 
+/* View-sharded reconstruction, the B200 form of the reference's MPY view
+ * split (Tomography_3D/Ytrtt3D_optim.i:48-124): one process per GPU, each
+ * with a plan of its own block of views (and its y, w); every rank runs the
+ * same iteration on a resident copy of the volume.  Per evaluation the
+ * ranks' data-term gradients (FP32 volume) and objectives (one FP64) are
+ * summed by `allreduce` (the regulariser is added by rank 0 only); the
+ * FP64 scalars the iteration branches on are averaged the same way, so all
+ * ranks take the same decisions.  allreduce(ctx, buf, count, dtype, stream)
+ * sums `count` device values in place over the ranks (dtype 0: float, 1:
+ * double) ordered on `stream`, and returns 0 (non-zero: the solve fails
+ * with -1).  world == 1 is trtt_b200_recon3d.  No counterpart in the
+ * reference's C. */
+typedef int (*trtt_b200_allreduce_fn)(void *ctx, void *buf, long count, int dtype, void *stream);
+int trtt_b200_recon3d_sharded(trtt_b200_plan3d *plan, const float *y, const float *w, float *x,
+                              int layout, double mu, double eps, double lower, double upper,
+                              int mem, int maxiter, double frtol, double *f_hist, double *t_hist,
+                              trtt_b200_vmlmb_info *info, void *stream, int rank, int world,
+                              trtt_b200_allreduce_fn allreduce, void *ctx);
+
 /* Allocation-free cone-beam direct projector.  No counterpart in the
  * reference (whose plugin allocates on the host per voxel).  For callers that
  * cannot call cudaMalloc: real-time or embedded hosts that forbid device

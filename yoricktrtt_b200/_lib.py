@@ -104,7 +104,12 @@ SIGNATURES = {
     "trtt_b200_plan3d_shape": (_I, [_vp, _lp]),
     "trtt_b200_recon3d": (_I, [_vp, _vp, _vp, _vp, _I, _D, _D, _D, _D, _I, _I, _D, _dp, _dp, _vp,
                                 _vp]),
+    "trtt_b200_recon3d_sharded": (_I, [_vp, _vp, _vp, _vp, _I, _D, _D, _D, _D, _I, _I, _D, _dp, _dp,
+                                        _vp, _vp, _I, _I, _vp, _vp]),
 }
+
+# trtt_b200_allreduce_fn: int (*)(void *ctx, void *buf, long count, int dtype, void *stream)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p)
 
 
 class VMLMBInfoC(C.Structure):

@@ -214,6 +214,21 @@ struct Solver {
   float *hx, *wr, *z, *tmp, *gz, *sg;
   long nviews;
   double *acc = nullptr;  // device scalars (kSlots)
+  // view sharding: this rank's data term is summed over `world` ranks by
+  // `allreduce` (one FP32 gradient and one FP64 objective per evaluation);
+  // the regulariser is added by rank 0 only, before the sum
+  int rank = 0, world = 1;
+  trtt_b200_allreduce_fn allreduce = nullptr;
+  void *ctx = nullptr;
+
+  // in-place sum over the ranks of `count` device values (dtype 0: FP32,
+  // 1: FP64); a no-op on one rank
+  int reduce(void *buf, long count, int dtype)
+  {
+    if (world <= 1) return 0;
+    if (allreduce(ctx, buf, count, dtype, st) != 0) return trtt::fail("recon3d: all-reduce failed");
+    return 0;
+  }
 
   // hand out the workspace's buffers in a fixed order; allocate on first use
   float *alloc(long count)
@@ -238,7 +253,7 @@ struct Solver {
     if (trtt_b200_wls_residual(hx, y, w, wr, m, acc + kF, st) != 0) return -1;
     TRTT_CK(cudaMemsetAsync(g, 0, sizeof(float) * n, st));
     if (trtt_b200_plan3d_backward(plan, wr, g, 0, nviews, TRTT_B200_LAYOUT_COLUMNS, st) != 0) return -1;
-    if (mu > 0) {
+    if (mu > 0 && rank == 0) {
       if (trtt_b200_spline_sample(x, z, tmp, tx, ty, tz, st) != 0) return -1;
       TRTT_CK(cudaMemsetAsync(gz, 0, sizeof(float) * n, st));
       if (trtt_b200_tv(z, tx, ty, tz, eps, mu, gz, acc + kF, st) != 0) return -1;
@@ -246,25 +261,31 @@ struct Solver {
       k_add<<<blocks_for(n), kThreads, 0, st>>>(g, sg, n);
       trtt::count_launch();
     }
+    if (reduce(g, n, 0) != 0 || reduce(acc + kF, 1, 1) != 0) return -1;
+    if (extra_dev && reduce(extra_dev, 1, 1) != 0) return -1;
     double h[1];
     TRTT_CK(cudaMemcpyAsync(h, acc + kF, sizeof(double), cudaMemcpyDeviceToHost, st));
     if (extra_dev) TRTT_CK(cudaMemcpyAsync(extra, extra_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
     TRTT_CK(cudaStreamSynchronize(st));
     *f = h[0];
+    if (extra_dev) *extra /= (double)world;  // the ranks' copies of a replicated value
     return 0;
   }
 };
 
 }  // namespace
 
-extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, float *x, int layout,
-                                 double mu, double eps, double lower, double upper, int mem, int maxiter,
-                                 double frtol, double *f_hist, double *t_hist, trtt_b200_vmlmb_info *info,
-                                 void *stream)
+extern "C" int trtt_b200_recon3d_sharded(trtt_b200_plan3d *plan, const float *y, const float *w, float *x,
+                                         int layout, double mu, double eps, double lower, double upper,
+                                         int mem, int maxiter, double frtol, double *f_hist, double *t_hist,
+                                         trtt_b200_vmlmb_info *info, void *stream, int rank, int world,
+                                         trtt_b200_allreduce_fn allreduce, void *ctx)
 {
   using namespace trtt;
   clear_error();
   if (!plan || !y || !x || !info) return fail("recon3d: null argument");
+  if (world < 1 || rank < 0 || rank >= world) return fail("recon3d: invalid rank / world");
+  if (world > 1 && !allreduce) return fail("recon3d: several ranks need an all-reduce hook");
   if (layout != TRTT_B200_LAYOUT_XYZ && layout != TRTT_B200_LAYOUT_COLUMNS)
     return fail("recon3d: unknown volume layout");
   if (mem < 1 || mem > 32 || maxiter < 0 || !(frtol >= 0) || mu < 0 || !(eps > 0))
@@ -307,6 +328,10 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
   S.w = w;
   S.mu = mu;
   S.eps = eps;
+  S.rank = rank;
+  S.world = world;
+  S.allreduce = allreduce;
+  S.ctx = ctx;
   if (!W.acc) TRTT_CK(cudaMalloc(&W.acc, sizeof(double) * kSlots));
   S.acc = W.acc;
   const long n = S.n;
@@ -370,9 +395,14 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
       k_mdot<<<B, kThreads, 0, st>>>(Sb[pend[k]], Yb[pend[k]], fr, n, A + kPairs + k);
       count_launch();
     }
+    // sharded: every rank holds the same vectors; the scalars the host
+    // branches on are averaged over the ranks so that all ranks take the
+    // same decisions
+    if (S.reduce(A + kPg, kPairs + np - kPg, 1) != 0) return -1;
     std::vector<double> h(kPairs + np);
     TRTT_CK(cudaMemcpyAsync(h.data(), A, sizeof(double) * (kPairs + np), cudaMemcpyDeviceToHost, st));
     TRTT_CK(cudaStreamSynchronize(st));
+    for (int k = kPg; k < kPairs + np; ++k) h[k] /= (double)world;
     const double pgn = std::sqrt(h[kPg]), xn = std::sqrt(h[kX]);
     std::vector<double> syf(h.begin() + kPairs, h.end());
     if (cand >= 0) {
@@ -433,8 +463,10 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
       alpha = (xn > 0 ? 0.1 * xn : 1.0) / pgn;
     }
     double gd;
+    if (S.reduce(A + kGD, 1, 1) != 0) return -1;
     TRTT_CK(cudaMemcpyAsync(&gd, A + kGD, sizeof(double), cudaMemcpyDeviceToHost, st));
     TRTT_CK(cudaStreamSynchronize(st));
+    gd /= (double)world;
     if (gd >= 0.0 && have_dir) {  // not a descent direction: restart with the gradient
       for (int s : ring) freeslots.push_back(s);
       ring.clear();
@@ -442,8 +474,10 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
       k_dir<<<B, kThreads, 0, st>>>(d, pg, nullptr, g, n, A + kGD);
       count_launch();
       alpha = (xn > 0 ? 0.1 * xn : 1.0) / pgn;
+      if (S.reduce(A + kGD, 1, 1) != 0) return -1;
       TRTT_CK(cudaMemcpyAsync(&gd, A + kGD, sizeof(double), cudaMemcpyDeviceToHost, st));
       TRTT_CK(cudaStreamSynchronize(st));
+      gd /= (double)world;
     }
     // the step of this iteration goes to a free slot (it becomes the candidate pair)
     const int slot = freeslots.back();
@@ -499,4 +533,13 @@ extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const f
   TRTT_CK(cudaStreamSynchronize(st));
   info->seconds = seconds();
   return 0;
+}
+
+extern "C" int trtt_b200_recon3d(trtt_b200_plan3d *plan, const float *y, const float *w, float *x, int layout,
+                                 double mu, double eps, double lower, double upper, int mem, int maxiter,
+                                 double frtol, double *f_hist, double *t_hist, trtt_b200_vmlmb_info *info,
+                                 void *stream)
+{
+  return trtt_b200_recon3d_sharded(plan, y, w, x, layout, mu, eps, lower, upper, mem, maxiter, frtol,
+                                   f_hist, t_hist, info, stream, 0, 1, nullptr, nullptr);
 }

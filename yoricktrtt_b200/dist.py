@@ -13,6 +13,7 @@ nothing.
 """
 from __future__ import annotations
 
+import traceback
 from dataclasses import dataclass
 
 
@@ -57,3 +58,115 @@ class ShardedPair:
             dist.all_reduce(f, group=self.group)
             dist.all_reduce(g, group=self.group)
         return float(f.item()), g
+
+
+class _DeviceArray:
+    """A device buffer seen through the CUDA array interface (zero copy)."""
+
+    def __init__(self, ptr: int, count: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+def allreduce_hook(group=None):
+    """A trtt_b200_allreduce_fn that sums a device buffer over the ranks of
+    a torch.distributed group: NCCL on the buffer itself, or (gloo) through
+    a host copy.  Keep the returned object alive while the solver runs."""
+    import torch
+    import torch.distributed as dist
+    from . import _lib
+    backend = dist.get_backend(group)
+
+    def fn(ctx, buf, count, dtype, stream):
+        try:
+            dev = torch.cuda.current_device()
+            arr = _DeviceArray(buf, count, "<f4" if dtype == 0 else "<f8")
+            t = torch.as_tensor(arr, device=torch.device("cuda", dev))
+            if backend == "nccl":
+                dist.all_reduce(t, group=group)
+            else:
+                h = t.cpu()
+                dist.all_reduce(h, group=group)
+                t.copy_(h)
+            return 0
+        except Exception:  # reported by the solver as a failed all-reduce
+            traceback.print_exc()
+            return 1
+
+    return _lib.ALLREDUCE_FN(fn)
+
+
+def vmlmb_native_sharded(proj, y, w=None, x0=None, mu=0.0, eps=1e-3, lower=0.0, upper=None, mem=5,
+                         maxiter=100, frtol=1e-6, layout="xyz", group=None):
+    """recon.vmlmb_native over the views of all ranks of `group` (one
+    process per GPU): `proj`, `y` and `w` hold this rank's block of views
+    (shard_views), x0 the same start on every rank.  Every rank returns the
+    same iterate.  Returns (x, VMLMBInfo)."""
+    import ctypes as C
+    import math
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from . import _lib
+    from .projectors import LAYOUTS
+    from .recon import VMLMBInfo, _REASONS
+    if proj.nt != 1:
+        raise ValueError("vmlmb_native_sharded: gated (4D) projectors are not supported")
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    shape = proj.volume_shape(layout)
+    x = (torch.zeros(shape, device=y.device) if x0 is None else x0).clone().contiguous()
+    if tuple(x.shape) != tuple(shape) or x.dtype != torch.float32:
+        raise ValueError(f"x0 must be float32 with shape {tuple(shape)}")
+    y = y.contiguous()
+    w = None if w is None else w.contiguous()
+    fh = np.zeros(maxiter + 1)
+    th = np.zeros(maxiter + 1)
+    info_c = _lib.VMLMBInfoC()
+    hook = allreduce_hook(group) if world > 1 else None
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    rc = _lib.load().trtt_b200_recon3d_sharded(
+        proj._h, ptr(y), ptr(w) if w is not None else None, ptr(x), LAYOUTS[layout], float(mu),
+        float(eps), -math.inf if lower is None else float(lower),
+        math.inf if upper is None else float(upper), int(mem), int(maxiter), float(frtol),
+        fh.ctypes.data_as(C.POINTER(C.c_double)), th.ctypes.data_as(C.POINTER(C.c_double)),
+        C.byref(info_c), st, rank, world, C.cast(hook, C.c_void_p) if hook else None, None)
+    _lib.check(rc, "trtt_b200_recon3d_sharded")
+    k = info_c.iterations
+    info = VMLMBInfo(iterations=k, evaluations=info_c.evaluations, f=fh[:k + 1].tolist(),
+                     times=th[:k + 1].tolist(), converged=info_c.converged > 0,
+                     reason=_REASONS.get(info_c.converged, ""))
+    return x, info
+
+
+def sharded_fg(data_fg, reg_fg=None, group=None, rank: int | None = None):
+    """fg(x) of a view-sharded objective for an iteration run identically on
+    every rank: the rank's data term (value, gradient) summed over the ranks
+    by one all-reduce of the gradient and one of the value, plus the
+    regulariser, evaluated by rank 0 before the sum (the same split as
+    trtt_b200_recon3d_sharded).  Works with torch tensors on any device whose
+    backend the group uses; numpy arrays are converted."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    if rank is None:
+        rank = dist.get_rank(group) if dist.is_initialized() else 0
+
+    def fg(x):
+        f, g = data_fg(x)
+        numpy_in = isinstance(g, np.ndarray)
+        gt = torch.from_numpy(np.array(g, dtype=np.float64)) if numpy_in else g.clone()
+        if reg_fg is not None and rank == 0:
+            fr, gr = reg_fg(x)
+            f = f + fr
+            gt += torch.from_numpy(np.asarray(gr, dtype=np.float64)) if numpy_in else gr
+        ft = torch.tensor([float(f)], dtype=torch.float64, device=gt.device)
+        if dist.is_initialized():
+            dist.all_reduce(gt, group=group)
+            dist.all_reduce(ft, group=group)
+        return float(ft.item()), (gt.numpy() if numpy_in else gt)
+
+    return fg
