@@ -182,3 +182,31 @@ def test_dd2d_gpu_source_plane():
     with pytest.raises(_lib.TrttError):
         dropin.dd2d(out, np.ones((10, 10)), sc, 0)
     assert np.all(out == 0.5)
+
+
+# launch paths of the fan-beam direct kernel: a second grid row of cell
+# blocks (more than 1024 detector cells), the shared-memory table above
+# 48 KB (opt-in), and the per-cell kernel when the table would exceed 200 KB
+FAN_PATHS = [
+    ("cell_blocks", dict(nx=8, ny=6, nv=1500, s=1.0, v=0.05, views=3)),
+    ("table_above_48k", dict(nx=3200, ny=4, nv=160, s=0.1, v=3.0, views=4)),
+    ("per_cell_fallback", dict(nx=13000, ny=2, nv=120, s=0.02, v=3.0, views=4)),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", FAN_PATHS)
+def test_dd2d_gpu_fan_launch_paths(name, kw):
+    from yoricktrtt_b200 import dropin
+    k = dict(kw)
+    views = k.pop("views")
+    sc = _scan(G.TRTT_FAN_BEAM, k["nx"], k["ny"], k["nv"], k["s"], k["v"], views=views,
+               rsc=600.0, rsd=900.0)
+    rng = np.random.default_rng(21)
+    img = rng.random((sc.ny, sc.nx))
+    ref = _oracle(D.dd2d, sc, img, 0)
+    assert np.abs(ref).max() > 0, name
+    pre = rng.random(ref.shape)
+    out = pre.copy()
+    dropin.dd2d(out, np.ascontiguousarray(img), sc, 0)
+    assert _relmax(out - pre, ref) <= 1e-12, name
