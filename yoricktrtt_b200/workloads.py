@@ -157,12 +157,18 @@ def cone3d_recon(maxiter=100, frtol=1e-6, seed=0, n=256, nd=512, views=360):
     wall = time.perf_counter() - t0
     pr.status()
     err = float(torch.linalg.norm(x - truth) / torch.linalg.norm(truth))
+    f = np.asarray(info.f)
+    rel = np.abs(np.diff(f)) / np.maximum(np.abs(f[:-1]), np.abs(f[1:]))
+    first_below = {f"{t:g}": (int(np.argmax(rel <= t)) + 1 if np.any(rel <= t) else None)
+                   for t in (1e-2, 1e-3, 1e-4, 1e-5, 1e-6)}
     return {"config": f"3D cone {n}^3 -> {views} x {nd}^2, VMLM-B + TV (native solver) to {frtol:g} "
                       f"relative objective change, at most {maxiter} iterations",
             "iterations": info.iterations, "evaluations": info.evaluations,
             "converged": info.converged, "reason": info.reason, "seconds": wall,
             "ms_per_iteration": 1e3 * wall / max(1, info.iterations),
-            "f_first": info.f[0], "f_last": info.f[-1], "rel_err_vs_phantom": err}
+            "f_first": info.f[0], "f_last": info.f[-1], "rel_err_vs_phantom": err,
+            "first_iteration_with_relative_change_below": first_below,
+            "f_every_10": f[::10].tolist()}
 
 
 def gates4d(nt=10, seed=0, replays=5):
