@@ -271,7 +271,10 @@ int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
  * once for all members (group kernels).  counts[0..2] = singles, pairs and
  * quads found (all-zero when the group kernels never apply to the plan).
  * set_symmetry(plan, 0) returns to the per-view kernels (results equal to
- * FP32 summation order). */
+ * FP32 summation order); 1 (default) uses the group kernels; 2 the group
+ * kernels with the member profiles of the direct projector interleaved per
+ * detector cell and updated by plain shared-memory loads and stores
+ * wherever the voxels' first cells strictly increase along a column. */
 int trtt_b200_plan3d_groups(const trtt_b200_plan3d *plan, long *counts);
 int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *plan, int on);
 

@@ -35,11 +35,15 @@ CASES = {
     "u_tiles": (dict(nu=300, nv=70, us=0.15, vs=0.5, views=8), (0, 0, 2)),
     "u_tiles_3": (dict(nu=600, nv=40, us=0.08, vs=0.9, views=4), (0, 0, 1)),
     "bands": (dict(nu=48, nv=150, vs=0.2, views=8), (0, 0, 2)),
+    "coarse_u": (dict(nu=20, nv=36, us=2.0, views=8), (0, 0, 2)),  # < 1 cell per voxel
 }
 
 
 @pytest.mark.parametrize("case", list(CASES))
-def test_group_pair_matches_oracle(oracle_port, case):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_group_pair_matches_oracle(oracle_port, case, mode):
+    """mode 1: group kernels; mode 2: the direct group kernel with member
+    profiles interleaved per cell and plain updates on monotone columns."""
     import torch
     from yoricktrtt_b200.projectors import Projector3D
     kw, expect = CASES[case]
@@ -47,6 +51,7 @@ def test_group_pair_matches_oracle(oracle_port, case):
     name = "CB3D" if sc.mode == G.TRTT_CONE_BEAM else "PB3D"
     assert tuple(len([g for g in G.view_groups(sc) if len(g) == n]) for n in (1, 2, 4)) == expect
     pr = Projector3D(sc)
+    pr.set_symmetry(mode)
     assert pr.groups() == expect
     vol = np.ascontiguousarray(P.ellipsoids_3d(sc.nx, sc.ny, sc.nz, n=7, seed=3, dtype=np.float64))
     xt = torch.tensor(vol, dtype=torch.float32, device="cuda")

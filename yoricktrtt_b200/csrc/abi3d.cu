@@ -37,7 +37,7 @@ struct trtt_b200_plan3d {
   std::vector<View3D> hviews;
   // view groups related by turns of the grid (closed-form model, factorised
   // views): index 0 singles, 1 pairs (half turns), 2 quads (quarter turns)
-  bool sym = true;        // use the group kernels when they apply
+  int sym = 1;            // group kernels when they apply: 1, 2 (interleaved member profiles); 0 never
   bool grouped = false;   // groups were found (some group has 2 or 4 views)
   int ngroups[3] = {0, 0, 0};
   DevBuf groups[3];
@@ -245,7 +245,8 @@ extern "C" int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *pl, int on)
 {
   clear_error();
   if (!pl) return fail("plan3d_set_symmetry: null plan");
-  pl->sym = on != 0;
+  if (on < 0 || on > 2) return fail("plan3d_set_symmetry: mode must be 0, 1 or 2");
+  pl->sym = on;
   return 0;
 }
 
@@ -409,6 +410,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
       L.usplit = (P.nu + 255) / 256;
       L.utile = (P.nu + L.usplit - 1) / L.usplit;
       L.warps = 16;
+      L.interleave = pl->sym == 2 ? 1 : 0;
       L.err = pl->err.as<int>();
       TRTT_CK(launch_fwd3d_group(L, G, st));
       count_launch();

@@ -68,6 +68,7 @@ struct GroupFwdLaunch {
   int band_rows;         // R detector rows per CTA
   int usplit, utile;     // u tiles per band and cells per tile (utile <= 256)
   int warps;
+  int interleave = 0;    // 1: member profiles interleaved per cell, plain updates where they apply
   int *err;
 };
 

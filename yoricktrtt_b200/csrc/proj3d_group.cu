@@ -106,12 +106,56 @@ __device__ __forceinline__ void column_k_range(const ColGeo<MODEL_CUBIC> &c, dou
   khi = (int)kb;
 }
 
+// Add a[0..G) into the G interleaved member slots of one profile cell.
+template <int G>
+__device__ __forceinline__ void cell_add(float *cell, const float (&a)[G])
+{
+  if constexpr (G == 4) {
+    float4 *q = reinterpret_cast<float4 *>(cell);
+    float4 v = *q;
+    v.x += a[0];
+    v.y += a[1];
+    v.z += a[2];
+    v.w += a[3];
+    *q = v;
+  } else if constexpr (G == 2) {
+    float2 *q = reinterpret_cast<float2 *>(cell);
+    float2 v = *q;
+    v.x += a[0];
+    v.y += a[1];
+    *q = v;
+  } else {
+    *cell += a[0];
+  }
+}
+
+// True when floor(uc_k - hs_k), the first cell of voxel k's u-footprint
+// before any clamp, strictly increases or decreases along the column: the
+// voxels of one warp step then write distinct cells at every footprint
+// offset l, so a warp can update its profile with plain loads and stores.
+// |d uc/dk| = |B|; hs = hs0 h_u0 magn delta_u varies by at most
+// hs0 h_u0m |B| max|uc - a12| u_scl^2 inv_den per voxel.
+template <int GEOM>
+__device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D &V,
+                                                const ColGeo<MODEL_CUBIC> &c)
+{
+  const double b = fabs(c.B);
+  if constexpr (GEOM == GEOM_CONE) {
+    const double ua = c.A, ub = fma(c.B, (double)(P.nz - 1), c.A);
+    const double um = fmax(fabs(ua - V.a12), fabs(ub - V.a12));
+    const double dhs = P.hs0 * (double)c.h_u0m * b * um * P.u_scl * P.u_scl * (double)c.inv_den;
+    return b - dhs >= 1.002;
+  } else {
+    return b >= 1.002;
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Direct projector over view groups
 // ---------------------------------------------------------------------------
-template <int GEOM, int G>
+template <int GEOM, int G, bool IL>
 __global__ void __launch_bounds__(512, (G == 4 ? 1 : 2))
 k_fwd3d_group(const GroupFwdLaunch A)
 {
@@ -187,6 +231,81 @@ k_fwd3d_group(const GroupFwdLaunch A)
         column_k_range(cc, hsm, u0, u1, nz, klo, khi);
       }
       int lo = INT_MAX, hi = INT_MIN;
+      // interleaved profiles (IL): cell-major, the G member values of a cell
+      // side by side; member m of cell c at prof[c * G + m], else prof[m U + c]
+      const int cs = IL ? G : 1, ms = IL ? 1 : U;
+      if (IL && column_monotone<GEOM>(P, V, cc)) {
+        // plain loads and stores: every voxel walks its footprint from the
+        // unclamped first cell (where the primitive is 0), writing cells
+        // inside [u0, e); at each step the warp's 64 voxels write 64
+        // distinct cells, and the steps are ordered by __syncwarp
+        for (int kb = klo; kb < khi; kb += 64) {
+          const int k0 = kb + lane, k1 = k0 + 32;
+          float2 x[G];
+          bool any = false;
+#pragma unroll
+          for (int m = 0; m < G; ++m) {
+            x[m].x = (k0 < khi) ? __ldg(colp[m] + k0) : 0.0f;
+            x[m].y = (k1 < khi) ? __ldg(colp[m] + k1) : 0.0f;
+            any = any || x[m].x != 0.0f || x[m].y != 0.0f;
+          }
+          UPair up;
+          voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+          if (k0 >= khi || !any) up.n0 = 0;
+          if (k1 >= khi || !any) up.n1 = 0;
+          const double uc0 = fma(cc.B, (double)k0, cc.A), uc1 = fma(cc.B, (double)k1, cc.A);
+          const float2 hsv = mul2(make_float2(__frcp_rn(up.inc.x), __frcp_rn(up.inc.y)),
+                                  f2((float)P.hs0));
+          const int f0 = __double2int_rd(uc0 - (double)hsv.x), f1 = __double2int_rd(uc1 - (double)hsv.y);
+          // the reference's first cell is f clamped to [0, nu-1]: cells left
+          // of the tile are not written (c >= u0 below); a footprint that
+          // starts past the detector (f >= nu) gives its one clamped cell
+          // weight 0 - 0 and is dropped.  Where hs rounds f one cell away
+          // from the reference's lo, the cell between holds a weight below
+          // the primitive's value within 1e-6 of the support end (~1e-27).
+          const int e0 = up.n0 > 0 ? min(up.lo0 + up.n0, u1) : INT_MIN;
+          const int e1 = up.n1 > 0 ? min(up.lo1 + up.n1, u1) : INT_MIN;
+          const int L0 = (up.n0 > 0 && f0 < nu) ? max(e0 - f0, 0) : 0;
+          const int L1 = (up.n1 > 0 && f1 < nu) ? max(e1 - f1, 0) : 0;
+          const int Lw = __reduce_max_sync(FULLM, max(max(L0, L1), 0));
+          if (Lw <= 0) continue;
+          const float2 start = make_float2(fmaf((float)(f0 - up.lo0), up.inc.x, up.start.x),
+                                           fmaf((float)(f1 - up.lo1), up.inc.y, up.start.y));
+          float2 xr[G];
+#pragma unroll
+          for (int m = 0; m < G; ++m) xr[m] = mul2(x[m], up.rho);
+          float2 Fp = f2(0.0f);
+          float2 lf = f2(1.0f);
+          for (int l = 0; l < Lw; ++l) {
+            const float2 F = cubic_prim2(fma2(lf, up.inc, start));
+            const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+            const int c0 = f0 + l, c1 = f1 + l;
+            if (l < L0 && c0 >= u0) {
+              float a[G];
+#pragma unroll
+              for (int m = 0; m < G; ++m) a[m] = w.x * xr[m].x;
+              cell_add<G>(prof + (c0 - u0) * G, a);
+            }
+            if (l < L1 && c1 >= u0) {
+              float a[G];
+#pragma unroll
+              for (int m = 0; m < G; ++m) a[m] = w.y * xr[m].y;
+              cell_add<G>(prof + (c1 - u0) * G, a);
+            }
+            __syncwarp();
+            Fp = F;
+            lf = add2(lf, f2(1.0f));
+          }
+          if (L0 > 0 && e0 > max(f0, u0)) {
+            lo = min(lo, max(f0, u0));
+            hi = max(hi, e0);
+          }
+          if (L1 > 0 && e1 > max(f1, u0)) {
+            lo = min(lo, max(f1, u0));
+            hi = max(hi, e1);
+          }
+        }
+      } else
       for (int kb = klo; kb < khi; kb += 64) {
         const int k0 = kb + lane, k1 = k0 + 32;
         float2 x[G];
@@ -221,8 +340,8 @@ k_fwd3d_group(const GroupFwdLaunch A)
         float2 xr[G];
 #pragma unroll
         for (int m = 0; m < G; ++m) xr[m] = mul2(x[m], up.rho);
-        float *p0 = prof + (c0 - u0);
-        float *p1 = prof + (c1 - u0);
+        float *p0 = prof + (c0 - u0) * cs;
+        float *p1 = prof + (c1 - u0) * cs;
         float2 lf = f2(1.0f);
         for (int l = 0; l < L; ++l) {
           const float2 F = cubic_prim2(fma2(lf, up.inc, start));
@@ -230,8 +349,8 @@ k_fwd3d_group(const GroupFwdLaunch A)
 #pragma unroll
           for (int m = 0; m < G; ++m) {
             const float2 p = mul2(w, xr[m]);
-            if (l < n0) atomicAdd(p0 + m * U + l, p.x);
-            if (l < n1) atomicAdd(p1 + m * U + l, p.y);
+            if (l < n0) atomicAdd(p0 + m * ms + l * cs, p.x);
+            if (l < n1) atomicAdd(p1 + m * ms + l * cs, p.y);
           }
           Fp = F;
           lf = add2(lf, f2(1.0f));
@@ -252,6 +371,26 @@ k_fwd3d_group(const GroupFwdLaunch A)
         // spread: band_m[r][u] += wv[r] * P_m[u]; each profile read once
         // into registers (and cleared), one shared atomic per cell and row
         constexpr int CH = 8;  // U <= 256 cells per tile
+        float pvs[G][CH];
+        if constexpr (IL) {
+#pragma unroll
+          for (int q = 0; q < CH; ++q) {
+            const int u = lo + lane + 32 * q;
+            float a[G];
+#pragma unroll
+            for (int m = 0; m < G; ++m) a[m] = 0.f;
+            if (u < hi) {
+              float *cell = prof + (u - u0) * G;
+#pragma unroll
+              for (int m = 0; m < G; ++m) {
+                a[m] = cell[m];
+                cell[m] = 0.f;
+              }
+            }
+#pragma unroll
+            for (int m = 0; m < G; ++m) pvs[m][q] = a[m];
+          }
+        }
 #pragma unroll
         for (int m = 0; m < G; ++m) {
           float pv[CH];
@@ -259,10 +398,14 @@ k_fwd3d_group(const GroupFwdLaunch A)
 #pragma unroll
           for (int q = 0; q < CH; ++q) {
             const int u = lo + lane + 32 * q;
-            pv[q] = 0.f;
-            if (u < hi) {
-              pv[q] = pm[u - u0];
-              pm[u - u0] = 0.f;
+            if constexpr (IL) {
+              pv[q] = pvs[m][q];
+            } else {
+              pv[q] = 0.f;
+              if (u < hi) {
+                pv[q] = pm[u - u0];
+                pm[u - u0] = 0.f;
+              }
             }
           }
           float *bm = bands + (m * R + (rb - v0)) * U;
@@ -499,7 +642,7 @@ cudaError_t fwd_group(const GroupFwdLaunch &L, cudaStream_t st)
   const int nbands = (L.P.nv + L.band_rows - 1) / L.band_rows;
   dim3 grid(nbands * L.usplit, L.ngroups);
   const size_t smem = group_fwd_smem(G, L.band_rows, L.utile, L.warps);
-  auto kern = k_fwd3d_group<GEOM, G>;
+  auto kern = L.interleave ? k_fwd3d_group<GEOM, G, true> : k_fwd3d_group<GEOM, G, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<grid, L.warps * 32, smem, st>>>(L);

@@ -98,10 +98,12 @@ class Projector3D:
                    "trtt_b200_plan3d_set_tiles")
         _lib.check(lib.trtt_b200_plan3d_set_columns(self._h, cols), "trtt_b200_plan3d_set_columns")
 
-    def set_symmetry(self, on: bool = True) -> None:
+    def set_symmetry(self, on=True) -> None:
         """Use (default) or bypass the group kernels that share footprints
-        between views related by turns of the volume grid."""
-        _lib.check(_lib.load().trtt_b200_plan3d_set_symmetry(self._h, 1 if on else 0),
+        between views related by turns of the volume grid; on=2 selects the
+        direct group kernel with interleaved member profiles."""
+        mode = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        _lib.check(_lib.load().trtt_b200_plan3d_set_symmetry(self._h, mode),
                    "trtt_b200_plan3d_set_symmetry")
 
     def groups(self):

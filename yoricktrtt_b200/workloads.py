@@ -319,12 +319,12 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     pr = Projector3D(sc)
     if tiles:
         pr.set_tiles(*tiles)
-    pr.set_symmetry(bool(sym))
+    pr.set_symmetry(int(sym))
     x = columns_from_xyz(torch.tensor(vol, device="cuda"))
     y = torch.zeros(pr.detector_shape(), device="cuda")
     b = torch.zeros_like(x)
     res = {"config": f"cone {n}x{n}x{nz} -> {views} x {nd}^2, cubic, {'dense' if dense else 'phantom'}",
-           "groups": pr.groups(), "symmetry": bool(sym)}
+           "groups": pr.groups(), "symmetry": int(sym)}
     for _ in range(reps):
         if direct:
             a, e = _events()
