@@ -36,6 +36,7 @@ CASES = {
     "u_tiles_3": (dict(nu=600, nv=40, us=0.08, vs=0.9, views=4), (0, 0, 1)),
     "bands": (dict(nu=48, nv=150, vs=0.2, views=8), (0, 0, 2)),
     "coarse_u": (dict(nu=20, nv=36, us=2.0, views=8), (0, 0, 2)),  # < 1 cell per voxel
+    "odd_nu": (dict(nu=42, nv=37, views=8), (0, 0, 2)),  # scalar profile loads
 }
 
 

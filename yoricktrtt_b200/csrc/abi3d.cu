@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -427,6 +428,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
       L.sino = src;
       L.sino_view_stride = npix;
       L.vol = volo;
+      L.vec4 = (P.nu % 4 == 0 && ((uintptr_t)src & 15) == 0) ? 1 : 0;
       L.err = pl->err.as<int>();
       // groups per launch: the launch's detector images stay in L2 while
       // every orbit walks them
@@ -680,6 +682,7 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
     L.sino = D.det32.as<float>();
     L.sino_view_stride = nview_px;
     L.vol = D.vol32.as<float>();
+    L.vec4 = (nu % 4 == 0) ? 1 : 0;  // det32 comes from cudaMalloc
     L.err = D.err.as<int>();
     const std::vector<long> cb = back_chunks(n, std::max<long>(1, n / 32), (n + 5) / 6, 10);
     for (size_t c = 0; c + 1 < cb.size(); ++c) {

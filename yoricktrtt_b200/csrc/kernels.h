@@ -83,6 +83,7 @@ struct GroupBackLaunch {
   const float *sino;     // [view][nv][nu], all views of the plan
   long sino_view_stride;
   float *vol;            // column layout, accumulated
+  int vec4 = 0;          // 1: nu % 4 == 0 and sino 16-byte aligned (vector loads)
   int *err;
 };
 

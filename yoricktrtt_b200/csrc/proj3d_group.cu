@@ -547,6 +547,48 @@ k_back3d_group(const GroupBackLaunch A)
         if (lo >= hi) continue;
         // v-collapsed profiles of the member views over cells [lo, hi)
         const int npv = cc.vax.n;
+        if (A.vec4) {
+          // 16-byte loads of four cells and packed FMAs over the aligned
+          // cover [lo & ~3, hi rounded up to 4) (nu % 4 == 0: rows and Q are
+          // 16-byte aligned; the padding cells of Q are never read)
+          constexpr int QV = G == 4 ? 1 : 2;  // float4 chunks per lane
+          const int a0 = lo & ~3, a1 = (hi + 3) & ~3;
+          for (int ub = a0; ub < a1; ub += 128 * QV) {
+            float4 q[G][QV];
+#pragma unroll
+            for (int m = 0; m < G; ++m)
+#pragma unroll
+              for (int c = 0; c < QV; ++c) q[m][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int m0 = 0; m0 < npv; m0 += 32) {
+              const int mn = min(32, npv - m0);
+              const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+              for (int rr = 0; rr < mn; ++rr) {
+                const float2 w = f2(__shfl_sync(FULLM, wl, rr));
+                const long roff = (long)(cc.vax.lo + m0 + rr) * nu + ub + 4 * lane;
+#pragma unroll
+                for (int m = 0; m < G; ++m) {
+                  const float4 *row = reinterpret_cast<const float4 *>(img[m] + roff);
+#pragma unroll
+                  for (int c = 0; c < QV; ++c) {
+                    if (ub + 4 * lane + 128 * c < a1) {
+                      const float4 y = __ldg(row + 32 * c);
+                      const float2 lo2 = fma2(w, make_float2(y.x, y.y), make_float2(q[m][c].x, q[m][c].y));
+                      const float2 hi2 = fma2(w, make_float2(y.z, y.w), make_float2(q[m][c].z, q[m][c].w));
+                      q[m][c] = make_float4(lo2.x, lo2.y, hi2.x, hi2.y);
+                    }
+                  }
+                }
+              }
+            }
+#pragma unroll
+            for (int m = 0; m < G; ++m)
+#pragma unroll
+              for (int c = 0; c < QV; ++c) {
+                const int u = ub + 4 * lane + 128 * c;
+                if (u < a1) *reinterpret_cast<float4 *>(Q + m * nu + u) = q[m][c];
+              }
+          }
+        } else {
         constexpr int QC = G == 4 ? 4 : 8;
         for (int ub = lo; ub < hi; ub += 32 * QC) {
           float q[G][QC];
@@ -576,6 +618,7 @@ k_back3d_group(const GroupBackLaunch A)
 #pragma unroll
             for (int c = 0; c < QC; ++c)
               if (ub + lane + 32 * c < hi) Q[m * nu + ub + lane + 32 * c] = q[m][c];
+        }
         }
         __syncwarp();
         // per-voxel gathers, two voxels per instruction; member m's sum goes
@@ -658,6 +701,7 @@ cudaError_t back_group(const GroupBackLaunch &L, cudaStream_t st)
   dim3 grid((L.norbits + warps - 1) / warps, (L.P.nz + 64 * KP - 1) / (64 * KP));
   const size_t smem = sizeof(float) * (size_t)warps * G * L.P.nu;
   auto kern = k_back3d_group<GEOM, G, KP>;
+  // L.vec4 set by the caller: nu % 4 == 0 and 16-byte aligned images
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<grid, warps * 32, smem, st>>>(L);
