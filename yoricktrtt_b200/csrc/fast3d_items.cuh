@@ -136,22 +136,26 @@ __device__ __forceinline__ void band_item(const Params3D &P, const View3D &V,
 // persistent kernel.
 struct LoadNC {
   __device__ __forceinline__ static float ld(const float *p) { return __ldg(p); }
+  __device__ __forceinline__ static float4 ld4(const float4 *p) { return __ldg(p); }
 };
 struct LoadCG {
   __device__ __forceinline__ static float ld(const float *p) { return __ldcg(p); }
+  __device__ __forceinline__ static float4 ld4(const float4 *p) { return __ldcg(p); }
 };
 
 // Column item.  One warp: column col = (i, j), voxels kbase + lane + 64 p
 // (+32), p < KP, gate `gate`; the entries [e0, e1) of the gate's list with
 // views in [view_lo, view_hi) (images at sino[view - view_lo]).  Q: this
-// warp's nu floats.  Adds the result into vol (one owner per voxel).
+// warp's nu floats.  vec4: nu % 4 == 0 and 16-byte aligned images (the
+// profile is then built from 16-byte loads).  Adds the result into vol (one
+// owner per voxel).
 template <int GEOM, int KP, class LD>
 __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__restrict__ views,
                                             const GateEntry *__restrict__ entries, int e0, int e1,
                                             int view_lo, int view_hi, const float *sino,
                                             long sino_view_stride, float *__restrict__ vol,
                                             long gate_stride, int col, int kbase, int gate, float *Q,
-                                            int *__restrict__ err)
+                                            int *__restrict__ err, bool vec4 = false)
 {
   const int lane = threadIdx.x & 31;
   const int nu = P.nu, nz = P.nz;
@@ -212,6 +216,40 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
       // so a warp keeps many loads in flight.
       const int npv = cc.vax.n;
       const float *img0 = sino + (long)(view - view_lo) * sino_view_stride;
+      if (vec4) {
+        // cover [lo & ~3, hi rounded up to 4): 16-byte loads, packed FMAs
+        constexpr int QV = 4;
+        const int a0 = lo & ~3, a1 = (hi + 3) & ~3;
+        for (int ub = a0; ub < a1; ub += 128 * QV) {
+          float4 q[QV];
+#pragma unroll
+          for (int c = 0; c < QV; ++c) q[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int m0 = 0; m0 < npv; m0 += 32) {
+            const int mn = min(32, npv - m0);
+            const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+            for (int m = 0; m < mn; ++m) {
+              const float2 w = f2(__shfl_sync(FULLM, wl, m));
+              const float4 *row =
+                  reinterpret_cast<const float4 *>(img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + 4 * lane);
+              float4 a[QV];
+#pragma unroll
+              for (int c = 0; c < QV; ++c)
+                a[c] = (ub + 4 * lane + 128 * c < a1) ? LD::ld4(row + 32 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+              for (int c = 0; c < QV; ++c) {
+                const float2 l2 = fma2(w, make_float2(a[c].x, a[c].y), make_float2(q[c].x, q[c].y));
+                const float2 h2 = fma2(w, make_float2(a[c].z, a[c].w), make_float2(q[c].z, q[c].w));
+                q[c] = make_float4(l2.x, l2.y, h2.x, h2.y);
+              }
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < QV; ++c) {
+            const int u = ub + 4 * lane + 128 * c;
+            if (u < a1) *reinterpret_cast<float4 *>(Q + u) = q[c];
+          }
+        }
+      } else {
       constexpr int QC = 16;
       for (int ub = lo; ub < hi; ub += 32 * QC) {
         float q[QC];
@@ -233,6 +271,7 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
 #pragma unroll
         for (int c = 0; c < QC; ++c)
           if (ub + lane + 32 * c < hi) Q[ub + lane + 32 * c] = q[c];
+      }
       }
       __syncwarp();
       // per-voxel gathers, two voxels per instruction

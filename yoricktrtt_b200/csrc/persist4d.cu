@@ -141,7 +141,8 @@ k_wls_persistent(const WlsLaunch A)
       if (col < ncols)
         column_item<GEOM, KP, LoadCG>(P, A.views, A.entries, A.gate_ptr[gate], A.gate_ptr[gate + 1],
                                       0, A.nviews, A.resid, (long)nu * nv, A.grad, A.gate_stride,
-                                      col, kc * (64 * KP), gate, sm + warp * nu, A.err);
+                                      col, kc * (64 * KP), gate, sm + warp * nu, A.err,
+                                      (nu & 3) == 0);
       __syncthreads();
     }
   }

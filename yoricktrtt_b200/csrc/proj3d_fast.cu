@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cstdint>
 
 #include "fast3d_items.cuh"
 #include "kernels.h"
@@ -340,7 +341,7 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
                   const int *__restrict__ gate_ptr, const GateEntry *__restrict__ entries,
                   int view_lo, int view_hi, const float *__restrict__ sino,
                   long sino_view_stride, float *__restrict__ vol, long gate_stride,
-                  int *__restrict__ err)
+                  int *__restrict__ err, int vec4)
 {
   extern __shared__ float sm[];
   const int nwarps = blockDim.x >> 5;
@@ -351,7 +352,7 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
   const int gate = blockIdx.z;
   column_item<GEOM, KP, LoadNC>(P, views, entries, gate_ptr[gate], gate_ptr[gate + 1], view_lo,
                                 view_hi, sino, sino_view_stride, vol, gate_stride, col,
-                                blockIdx.y * (64 * KP), gate, sm + warp * P.nu, err);
+                                blockIdx.y * (64 * KP), gate, sm + warp * P.nu, err, vec4 != 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -410,8 +411,11 @@ static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
   auto kern = k_back3d_col_fast<GEOM, KP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  // 16-byte profile loads: rows of nu % 4 == 0 floats in 16-byte aligned images
+  const int vec4 = (L.P.nu % 4 == 0 && L.sino_view_stride % 4 == 0 &&
+                    ((uintptr_t)L.sino & 15) == 0) ? 1 : 0;
   kern<<<grid, warps * 32, smem, st>>>(L.P, L.views, L.gate_ptr, L.entries, L.view_lo, L.view_hi,
-                                      L.sino, L.sino_view_stride, L.vol, L.gate_stride, L.err);
+                                      L.sino, L.sino_view_stride, L.vol, L.gate_stride, L.err, vec4);
   return cudaGetLastError();
 }
 
