@@ -511,6 +511,15 @@ int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, float *sino,
  * unet_status: -1 if a convolution kernel gave up waiting for its tensor-core
  *   work (bounded waits), then clears the flag; synchronises the stream. */
 int trtt_b200_conv3_pack(const float *w, int cout, int cin, int transpose, void *wpack, void *stream);
+/* Staging of trtt_b200_conv3_forward, process-wide: 0 (default) copies each
+ * stage's slab and weights into shared memory with 16-byte cp.async by all
+ * 128 threads; 1 loads them with TMA (2D tiled copies of the padded
+ * channels-last activations, a bulk copy of the weights) issued by one
+ * producer thread while one thread issues the MMAs on an mbarrier ring
+ * (warp specialisation).  Both compute the same MMAs in the same order
+ * (identical results).  -1 when the driver provides no tensor-map
+ * encoder.  No counterpart in the reference. */
+int trtt_b200_conv3_set_tma(int on);
 int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, const void *wpack, int n,
                             const float *bias, int mode, float slope, void *y, void *y2, int n1,
                             int accumulate, const float *resid, int nb, int d, int h, int w,

@@ -216,3 +216,74 @@ def test_unet_training_reduces_loss(lib):
     net.status()
     assert all(np.isfinite(losses))
     assert losses[-1] < 0.3 * losses[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c1,c2,co,dims", [(16, 0, 16, (2, 6, 10, 20)), (16, 32, 48, (1, 8, 12, 40)),
+                                           (64, 0, 64, (1, 4, 6, 130)), (32, 16, 96, (2, 6, 10, 20))])
+def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
+    """TMA staging with a producer thread and an MMA thread on an mbarrier
+    ring (trtt_b200_conv3_set_tma(1)) gives the same outputs as the cp.async
+    staging: the same MMAs in the same order.  The widths cover a slab of
+    one partial TMA box (w = 20), of several boxes (w = 130: 518 rows, two
+    full boxes of 256 and one of 6)."""
+    from yoricktrtt_b200._lib import check
+    from yoricktrtt_b200.unet import _p, _stream
+    g = torch.Generator().manual_seed(c1 + 3 * c2 + co)
+    nb, d, h, w = dims
+    x1 = _bf(torch.randn(nb, c1, d, h, w, generator=g))
+    x2 = _bf(torch.randn(nb, c2, d, h, w, generator=g)) if c2 else None
+    cin = c1 + c2
+    wt = torch.randn(co, 27, cin, generator=g) / np.sqrt(27 * cin)
+    bias = torch.randn(co, generator=g).cuda()
+    pack = torch.empty(27 * co * cin, dtype=torch.bfloat16, device="cuda")
+    check(lib.trtt_b200_conv3_pack(_p(wt.cuda()), co, cin, 0, _p(pack), _stream()), "pack")
+    xp1, xp2 = _padded(x1), (_padded(x2) if c2 else None)
+    rows = xp1.shape[0]
+    outs = []
+    try:
+        for tma in (0, 1):
+            check(lib.trtt_b200_conv3_set_tma(tma), "set_tma")
+            y = torch.zeros(rows, co, dtype=torch.float32, device="cuda")
+            check(lib.trtt_b200_conv3_forward(_p(xp1), c1, _p(xp2), c2, _p(pack), co, _p(bias), 1, 1.0,
+                                              _p(y), None, 0, 0, None, nb, d, h, w, _stream()), "conv")
+            yb = torch.zeros(rows, co, dtype=torch.bfloat16, device="cuda")
+            check(lib.trtt_b200_conv3_forward(_p(xp1), c1, _p(xp2), c2, _p(pack), co, _p(bias), 0, 0.1,
+                                              _p(yb), None, 0, 0, None, nb, d, h, w, _stream()), "conv")
+            check(lib.trtt_b200_unet_status(_stream()), "status")
+            outs.append((y.cpu(), yb.cpu()))
+    finally:
+        lib.trtt_b200_conv3_set_tma(0)
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
+    ref = _conv_ref(torch.cat([x1, x2], 1) if c2 else x1, _bf(wt), bias.double().cpu())
+    got = outs[1][0].reshape(nb, d + 2, h + 2, w + 2, co)[:, 1:-1, 1:-1, 1:-1].permute(0, 4, 1, 2, 3).double()
+    assert rel_l2(got.numpy(), ref.numpy()) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_unet_training_step_tma_staging():
+    """A U-Net forward and backward (input gradients run the same kernel)
+    with TMA staging equals the cp.async staging."""
+    from yoricktrtt_b200 import _lib
+    from yoricktrtt_b200.unet import UNet3D
+    lib = _lib.load()
+    x = torch.rand(1, 32, 32, 32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
+    t = torch.rand(1, 32, 32, 32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(2))
+    res = []
+    try:
+        for tma in (0, 1):
+            _lib.check(lib.trtt_b200_conv3_set_tma(tma), "set_tma")
+            net = UNet3D(seed=3)
+            y = net.forward(x).clone()
+            loss = net.backward(x, t)
+            net.status()
+            res.append((y.cpu(), float(loss),
+                        {(k, n): g.clone().cpu() for k, v in net._grads.items() for n, g in v.items()}))
+    finally:
+        lib.trtt_b200_conv3_set_tma(0)
+    assert torch.equal(res[0][0], res[1][0])
+    assert res[0][1] == res[1][1]
+    # weight gradients sum row-range partials in a fixed order: equal too
+    for key, g0 in res[0][2].items():
+        assert torch.equal(g0, res[1][2][key]), key

@@ -100,6 +100,7 @@ SIGNATURES = {
     "trtt_b200_adam": (_I, [_vp, _vp, _vp, _vp, _L, C.c_float, C.c_float, C.c_float, C.c_float,
                              _I, C.c_float, _vp]),
     "trtt_b200_unet_status": (_I, [_vp]),
+    "trtt_b200_conv3_set_tma": (_I, [_I]),
     "trtt_b200_unet_add_output_grad": (_I, [_vp, _vp, C.c_float, _I, _I, _I, _I, _vp]),
     "trtt_b200_plan3d_shape": (_I, [_vp, _lp]),
     "trtt_b200_recon3d": (_I, [_vp, _vp, _vp, _vp, _I, _D, _D, _D, _D, _I, _I, _D, _dp, _dp, _vp,

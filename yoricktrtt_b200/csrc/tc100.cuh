@@ -152,6 +152,32 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t parity, uint64_t
   return true;
 }
 
+// Tensor memory accelerator (TMA) -----------------------------------------
+// All copies here read this GPU's own global memory into this CTA's shared
+// memory (no cluster multicast).  Completion is signalled on an mbarrier as
+// transaction bytes.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *m, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)), "r"(bytes)
+               : "memory");
+}
+// 2D tiled load of the tensor map's box at element coordinates (x, y), x
+// the innermost dimension (x * element size a multiple of 16 bytes).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *tmap, int x, int y, uint64_t *mbar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_addr(mbar))
+      : "memory");
+}
+// Contiguous copy of `bytes` (a multiple of 16; both addresses 16-byte aligned).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint64_t *mbar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+               : "memory");
+}
+
 // cp.async ---------------------------------------------------------------
 // 16-byte global -> shared copy; `valid` false writes 16 zero bytes (the
 // source is not read).

@@ -34,11 +34,13 @@
 // Every wait on an mbarrier is bounded in time; a kernel that gives up sets
 // a device error word (read by trtt_b200_unet_status), drains its copies,
 // frees its tensor memory and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 
 #include "runtime.h"
 #include "tc100.cuh"
@@ -111,6 +113,75 @@ struct FwdArgs {
   int rh, cs, stage_bytes, nstg;
   uint32_t tmem_cols;
 };
+
+// Epilogue of the forward / input-gradient convolution: the S accumulators
+// of 128 rows x n columns in tensor memory (warp w reads TMEM lanes
+// 32w..32w+31) to bias, activation and the output layout of the mode.
+template <int S>
+__device__ __forceinline__ void fwd_epilogue(const FwdArgs &a, uint32_t tmem, long m0, int warp, int lane)
+{
+  const int n = a.n;
+#pragma unroll 1
+  for (int s = 0; s < S; ++s) {
+    const long p = m0 + 128 * s + 32 * warp + lane;
+    const bool inside = interior(a.g, p);
+#pragma unroll 1
+    for (int j = 0; j < n; j += 16) {
+      float v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(s * n + j), v);
+      if (!inside) continue;
+      if (a.bias && a.mode != kFwdGrad) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] += a.bias[j + i];
+      }
+      if (a.mode == kFwdAct) {
+        uint4 q0, q1;
+        q0.x = pack_bf16x2(act(v[0], a.slope), act(v[1], a.slope));
+        q0.y = pack_bf16x2(act(v[2], a.slope), act(v[3], a.slope));
+        q0.z = pack_bf16x2(act(v[4], a.slope), act(v[5], a.slope));
+        q0.w = pack_bf16x2(act(v[6], a.slope), act(v[7], a.slope));
+        q1.x = pack_bf16x2(act(v[8], a.slope), act(v[9], a.slope));
+        q1.y = pack_bf16x2(act(v[10], a.slope), act(v[11], a.slope));
+        q1.z = pack_bf16x2(act(v[12], a.slope), act(v[13], a.slope));
+        q1.w = pack_bf16x2(act(v[14], a.slope), act(v[15], a.slope));
+        uint4 *dst = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.y) + p * n + j);
+        dst[0] = q0;
+        dst[1] = q1;
+      } else if (a.mode == kFwdF32) {
+        float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(a.y) + p * n + j);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dst[i] = make_float4(act(v[4 * i], a.slope), act(v[4 * i + 1], a.slope),
+                               act(v[4 * i + 2], a.slope), act(v[4 * i + 3], a.slope));
+      } else if (a.mode == kFwdHead) {
+        if (j == 0) static_cast<float *>(a.y)[p] = a.resid[p] + v[0];
+      } else {  // kFwdGrad
+        bf16 *base;
+        int ld, c0;
+        if (j < a.n1) { base = static_cast<bf16 *>(a.y); ld = a.n1; c0 = j; }
+        else { base = static_cast<bf16 *>(a.y2); ld = n - a.n1; c0 = j - a.n1; }
+        uint4 *dst = reinterpret_cast<uint4 *>(base + p * ld + c0);
+        if (a.accumulate) {
+          const uint4 o0 = dst[0], o1 = dst[1];
+          const uint32_t ow[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const float2 f = unpack_bf16x2(ow[i]);
+            v[2 * i] += f.x;
+            v[2 * i + 1] += f.y;
+          }
+        }
+        uint4 q0, q1;
+        q0.x = pack_bf16x2(v[0], v[1]); q0.y = pack_bf16x2(v[2], v[3]);
+        q0.z = pack_bf16x2(v[4], v[5]); q0.w = pack_bf16x2(v[6], v[7]);
+        q1.x = pack_bf16x2(v[8], v[9]); q1.y = pack_bf16x2(v[10], v[11]);
+        q1.z = pack_bf16x2(v[12], v[13]); q1.w = pack_bf16x2(v[14], v[15]);
+        dst[0] = q0;
+        dst[1] = q1;
+      }
+    }
+  }
+}
 
 template <int S>
 __global__ void __launch_bounds__(128) k_conv3_fwd(const FwdArgs a)
@@ -192,69 +263,138 @@ __global__ void __launch_bounds__(128) k_conv3_fwd(const FwdArgs a)
 
   if (!bad) {
     tc::fence_after_sync();
-#pragma unroll 1
-    for (int s = 0; s < S; ++s) {
-      const long p = m0 + 128 * s + 32 * warp + lane;
-      const bool inside = interior(a.g, p);
-#pragma unroll 1
-      for (int j = 0; j < n; j += 16) {
-        float v[16];
-        tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(s * n + j), v);
-        if (!inside) continue;
-        if (a.bias && a.mode != kFwdGrad) {
-#pragma unroll
-          for (int i = 0; i < 16; ++i) v[i] += a.bias[j + i];
-        }
-        if (a.mode == kFwdAct) {
-          uint4 q0, q1;
-          q0.x = pack_bf16x2(act(v[0], a.slope), act(v[1], a.slope));
-          q0.y = pack_bf16x2(act(v[2], a.slope), act(v[3], a.slope));
-          q0.z = pack_bf16x2(act(v[4], a.slope), act(v[5], a.slope));
-          q0.w = pack_bf16x2(act(v[6], a.slope), act(v[7], a.slope));
-          q1.x = pack_bf16x2(act(v[8], a.slope), act(v[9], a.slope));
-          q1.y = pack_bf16x2(act(v[10], a.slope), act(v[11], a.slope));
-          q1.z = pack_bf16x2(act(v[12], a.slope), act(v[13], a.slope));
-          q1.w = pack_bf16x2(act(v[14], a.slope), act(v[15], a.slope));
-          uint4 *dst = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.y) + p * n + j);
-          dst[0] = q0;
-          dst[1] = q1;
-        } else if (a.mode == kFwdF32) {
-          float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(a.y) + p * n + j);
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            dst[i] = make_float4(act(v[4 * i], a.slope), act(v[4 * i + 1], a.slope),
-                                 act(v[4 * i + 2], a.slope), act(v[4 * i + 3], a.slope));
-        } else if (a.mode == kFwdHead) {
-          if (j == 0) static_cast<float *>(a.y)[p] = a.resid[p] + v[0];
-        } else {  // kFwdGrad
-          bf16 *base;
-          int ld, c0;
-          if (j < a.n1) { base = static_cast<bf16 *>(a.y); ld = a.n1; c0 = j; }
-          else { base = static_cast<bf16 *>(a.y2); ld = n - a.n1; c0 = j - a.n1; }
-          uint4 *dst = reinterpret_cast<uint4 *>(base + p * ld + c0);
-          if (a.accumulate) {
-            const uint4 o0 = dst[0], o1 = dst[1];
-            const uint32_t ow[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-              const float2 f = unpack_bf16x2(ow[i]);
-              v[2 * i] += f.x;
-              v[2 * i + 1] += f.y;
-            }
-          }
-          uint4 q0, q1;
-          q0.x = pack_bf16x2(v[0], v[1]); q0.y = pack_bf16x2(v[2], v[3]);
-          q0.z = pack_bf16x2(v[4], v[5]); q0.w = pack_bf16x2(v[6], v[7]);
-          q1.x = pack_bf16x2(v[8], v[9]); q1.y = pack_bf16x2(v[10], v[11]);
-          q1.z = pack_bf16x2(v[12], v[13]); q1.w = pack_bf16x2(v[14], v[15]);
-          dst[0] = q0;
-          dst[1] = q1;
-        }
-      }
-    }
+    fwd_epilogue<S>(a, tmem, m0, warp, lane);
   } else {
     tc::cp_wait_all();
     if (tid == 0) atomicExch(&g_unet_err, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, a.tmem_cols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forward / input-gradient convolution, TMA staging, warp-specialised
+// ---------------------------------------------------------------------------
+// Same GEMM, tile and stage layout as k_conv3_fwd, with the slab chunks at a
+// 128-byte-aligned stride.  One thread (warp 0) produces: per stage it waits
+// until the MMAs of the stage that last used the buffer have read it (the
+// buffer's `empty` barrier, signalled by tcgen05.commit), then loads the
+// two 8-channel chunks of the slab with 2D tiled TMA copies (boxes of 256
+// rows and one box of the remaining rows; rows outside the tensor read as
+// zeros) and the 9 weight tiles with one bulk copy, all completing on the
+// buffer's `full` barrier as transaction bytes.  One thread (warp 1) waits
+// on `full`, issues the stage's 9 S MMAs and commits them to `empty`; after
+// the last stage it commits to `acc`, on which every thread waits before
+// the epilogue.  The tensor maps cover only this GPU's memory; no copy uses
+// cluster multicast.  Every wait is bounded (2 s); a kernel that gives up
+// sets the error word, waits for its copies in flight, frees its tensor
+// memory and returns.
+struct FwdMaps {
+  CUtensorMap x1_full, x1_tail, x2_full, x2_tail;  // 8 channels x (256 | tail) rows
+  int tail;                                         // rows of the last box (0: none)
+};
+
+template <int S>
+__global__ void __launch_bounds__(128) k_conv3_fwd_tma(const FwdArgs a, const __grid_constant__ FwdMaps maps)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[4], empty[4], accb;
+  __shared__ uint32_t s_taddr;
+  __shared__ volatile int s_bad;
+  __shared__ int s_issued, s_consumed;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long m0 = a.row0 + (long)blockIdx.x * (128 * S);
+  const int T = 3 * a.groups, n = a.n, nstg = a.nstg;
+  const uint32_t sbase = tc::smem_addr(smem);
+
+  if (tid == 0) {
+    for (int i = 0; i < nstg; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    tc::mbar_init(&accb, 1);
+    s_bad = 0;
+    s_issued = 0;
+    s_consumed = 0;
+    tc::mbar_fence_init();
+  }
+  if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = s_taddr;
+  const uint32_t stage_tx = (uint32_t)(2 * a.rh * 16 + 288 * n);
+
+  if (tid == 0) {
+    // producer
+    int it = 0;
+    for (; it < T; ++it) {
+      const int slot = it % nstg;
+      if (it >= nstg && !tc::mbar_wait(&empty[slot], ((it / nstg) - 1) & 1, kWaitNs)) {
+        s_bad = 1;
+        break;
+      }
+      if (s_bad) break;
+      const int dz = it / a.groups - 1, ch = (it % a.groups) * 16;
+      const bool first = ch < a.c1;
+      const int coff = first ? ch : ch - a.c1;
+      const CUtensorMap *mfull = first ? &maps.x1_full : &maps.x2_full;
+      const CUtensorMap *mtail = first ? &maps.x1_tail : &maps.x2_tail;
+      const long hb = m0 + (long)dz * a.g.plane - a.g.wp - 1;
+      const uint32_t hs = sbase + (uint32_t)(slot * a.stage_bytes);
+      tc::mbar_arrive_expect_tx(&full[slot], stage_tx);
+      for (int c = 0; c < 2; ++c) {
+        for (int r0 = 0; r0 < a.rh; r0 += 256) {
+          const bool whole = a.rh - r0 >= 256;
+          tc::tma_load_2d(hs + (uint32_t)(c * a.cs + r0 * 16), whole ? mfull : mtail, coff + 8 * c,
+                          (int)(hb + r0), &full[slot]);
+        }
+      }
+      tc::bulk_load(hs + 2u * a.cs, a.wpack + (long)it * 9 * n * 16, (uint32_t)(288 * n), &full[slot]);
+    }
+    s_issued = it;
+  } else if (tid == 32) {
+    // MMA issuer
+    const uint32_t idesc = tc::idesc_bf16(128, n, 0, 0);
+    int it = 0;
+    for (; it < T; ++it) {
+      const int slot = it % nstg;
+      if (!tc::mbar_wait(&full[slot], (it / nstg) & 1, kWaitNs)) {
+        s_bad = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t hs = sbase + (uint32_t)(slot * a.stage_bytes), ws = hs + 2u * a.cs;
+      for (int t9 = 0; t9 < 9; ++t9) {
+        const int dy = t9 / 3, dx = t9 - 3 * (t9 / 3);
+        const uint64_t bd = tc::sdesc(ws + (uint32_t)(t9 * n * 32), (uint32_t)(n * 16), 128u);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const uint64_t ad = tc::sdesc(hs + (uint32_t)((dy * a.g.wp + dx + 128 * s) * 16), (uint32_t)a.cs, 128u);
+          tc::mma_bf16(tmem + (uint32_t)(s * n), ad, bd, idesc, (it > 0 || t9 > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&empty[slot]);
+    }
+    tc::mma_commit(&accb);  // arrives once every MMA issued above has completed
+    s_consumed = it;
+  }
+  const bool acc_ok = tc::mbar_wait(&accb, 0, kWaitNs);
+  __syncthreads();
+  const bool bad = __syncthreads_or(!acc_ok || s_bad);
+  if (!bad) {
+    tc::fence_after_sync();
+    fwd_epilogue<S>(a, tmem, m0, warp, lane);
+  } else {
+    if (tid == 0) {
+      // copies issued for stages the MMAs never consumed
+      for (int it = s_consumed; it < s_issued; ++it) tc::mbar_wait(&full[it % nstg], (it / nstg) & 1, kWaitNs);
+      atomicExch(&g_unet_err, 1);
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -734,6 +874,57 @@ FwdPlan fwd_plan(int n, int groups, const Grid3 &g)
   return p;
 }
 
+// Stage layout of the TMA forward kernel: as fwd_plan with the chunk stride
+// a multiple of 128 bytes (TMA writes shared memory at 128-byte-aligned
+// addresses).
+FwdPlan fwd_plan_tma(int n, int groups, const Grid3 &g)
+{
+  FwdPlan p = fwd_plan(n, groups, g);
+  p.cs = ((p.rh * 16 + 127) / 128) * 128;
+  p.stage_bytes = ((2 * p.cs + 288 * n + 1023) / 1024) * 1024;
+  p.nstg = (3 * groups <= 3 || 4 * p.stage_bytes > 112 * 1024) ? 3 : 4;
+  p.smem = residency_smem(p.nstg * p.stage_bytes, p.tmem_cols);
+  return p;
+}
+
+// cuTensorMapEncodeTiled, reached through the runtime (no driver library
+// link); null when the driver does not provide it.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
+{
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// Tensor map of a padded channels-last activation (rows x c BF16): boxes of
+// 8 channels x box_rows rows, zeros outside the tensor.
+bool act_map(CUtensorMap *m, const void *base, int c, long rows, int box_rows)
+{
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)c, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)c * 2};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int g_conv_tma = 0;  // trtt_b200_conv3_set_tma
+
 // Stage layout of the weight-gradient kernel: 256 rows per stage when two
 // CTAs still fit on an SM, else 128; row ranges split into chunks so that
 // the grid (9 x chunks) fills about four waves of resident CTAs, each CTA
@@ -819,6 +1010,32 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   a.resid = resid;
   a.g = make_grid(nb, d, h, w);
   a.row0 = a.g.plane;
+  if (g_conv_tma) {
+    const FwdPlan pl = fwd_plan_tma(n, a.groups, a.g);
+    a.rh = pl.rh;
+    a.cs = pl.cs;
+    a.stage_bytes = pl.stage_bytes;
+    a.nstg = pl.nstg;
+    a.tmem_cols = pl.tmem_cols;
+    if (pl.smem > 227 * 1024) return fail("conv3_forward: volume rows too long for the staged slab");
+    if (pl.tiles <= 0 || pl.tiles > 0x7FFFFFFFL) return fail("conv3_forward: bad tile count");
+    if ((reinterpret_cast<uintptr_t>(x1) & 15) || (c2 && (reinterpret_cast<uintptr_t>(x2) & 15)) ||
+        (reinterpret_cast<uintptr_t>(wpack) & 15))
+      return fail("conv3_forward: TMA staging needs 16-byte aligned tensors");
+    FwdMaps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    maps.tail = pl.rh % 256;
+    const int tail = maps.tail ? maps.tail : 256;
+    bool ok = act_map(&maps.x1_full, x1, c1, a.g.rows, 256) && act_map(&maps.x1_tail, x1, c1, a.g.rows, tail);
+    if (c2) ok = ok && act_map(&maps.x2_full, x2, c2, a.g.rows, 256) && act_map(&maps.x2_tail, x2, c2, a.g.rows, tail);
+    if (!ok) return fail("conv3_forward: tensor map encoding failed");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TRTT_CK(set_smem(k_conv3_fwd_tma<S>, pl.smem));
+    k_conv3_fwd_tma<S><<<(unsigned)pl.tiles, 128, pl.smem, st>>>(a, maps);
+    count_launch();
+    TRTT_CK(cudaGetLastError());
+    return 0;
+  }
   const FwdPlan pl = fwd_plan(n, a.groups, a.g);
   a.rh = pl.rh;
   a.cs = pl.cs;
@@ -834,6 +1051,15 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   k_conv3_fwd<S><<<(unsigned)tiles, 128, smem, st>>>(a);
   count_launch();
   TRTT_CK(cudaGetLastError());
+  return 0;
+}
+
+int trtt_b200_conv3_set_tma(int on)
+{
+  using namespace trtt;
+  clear_error();
+  if (on && !encode_tiled()) return fail("conv3_set_tma: the driver provides no tensor-map encoder");
+  g_conv_tma = on ? 1 : 0;
   return 0;
 }
 
