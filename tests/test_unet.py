@@ -264,7 +264,8 @@ def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
 @pytest.mark.gpu
 def test_unet_training_step_tma_staging():
     """A U-Net forward and backward (input gradients run the same kernel)
-    with TMA staging equals the cp.async staging."""
+    with TMA staging: the same forward output as the cp.async staging, the
+    same loss and gradients to summation order."""
     from yoricktrtt_b200 import _lib
     from yoricktrtt_b200.unet import UNet3D
     lib = _lib.load()
@@ -283,7 +284,8 @@ def test_unet_training_step_tma_staging():
     finally:
         lib.trtt_b200_conv3_set_tma(0)
     assert torch.equal(res[0][0], res[1][0])
-    assert res[0][1] == res[1][1]
-    # weight gradients sum row-range partials in a fixed order: equal too
+    # the loss and the bias gradients are sums with float atomics: equal to
+    # FP32 summation order
+    assert abs(res[0][1] - res[1][1]) <= 1e-6 * abs(res[0][1])
     for key, g0 in res[0][2].items():
-        assert torch.equal(g0, res[1][2][key]), key
+        assert rel_l2(res[1][2][key].double().numpy(), g0.double().numpy()) <= 1e-5, key
