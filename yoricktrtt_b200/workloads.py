@@ -345,17 +345,21 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     return res
 
 
-def unet_case(size=128, batch=1, reps=1, train=1, seed=0):
+def unet_case(size=128, batch=1, reps=1, train=1, tma=0, seed=0):
     """One U-Net case for profiling the tensor-core convolutions: ``reps``
     forward passes (and training steps when ``train``) on a batch of
-    size^3 inputs; returns the CUDA-event time of the last of each."""
+    size^3 inputs; returns the CUDA-event time of the last of each.
+    ``tma=1`` stages the forward / input-gradient convolutions with TMA."""
     torch = _torch()
+    from . import _lib
     from .unet import UNet3D
+    _lib.check(_lib.load().trtt_b200_conv3_set_tma(int(tma)), "trtt_b200_conv3_set_tma")
     net = UNet3D(seed=seed)
     g = torch.Generator(device="cuda").manual_seed(seed)
     x = torch.rand(batch, size, size, size, device="cuda", generator=g)
     t = torch.rand(batch, size, size, size, device="cuda", generator=g)
-    res = {"config": f"U-Net 3 levels 16/32/64, batch {batch} x {size}^3"}
+    res = {"config": f"U-Net 3 levels 16/32/64, batch {batch} x {size}^3, "
+                     f"{'TMA' if tma else 'cp.async'} staging"}
     for _ in range(reps):
         a, e = _events()
         a.record()
