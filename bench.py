@@ -403,6 +403,19 @@ def run_b200(args):
         parity = parity_block(pr, sc, vol_h, sino)
     barrier()
 
+    # the same pair with the per-view kernels (no footprint sharing between
+    # views related by turns of the grid), for comparison
+    per_view = None
+    if not args.skip_dense and not args.no_symmetry and sum(pr.groups()[1:]) > 0:
+        pr.set_symmetry(False)
+        psteps = max(1, min(args.steps, 2))
+        pms, pfwd, pback, _ = timed_pairs(pr, x, sino, back, flush, psteps, 1, world, barrier)
+        pms = max_over_ranks(pms)
+        per_view = {"value": 2 * VIEWS * world * psteps / (pms / 1e3), "unit": "projections/s",
+                    "fwd_ms": statistics.mean(pfwd), "back_ms": statistics.mean(pback),
+                    "steps": psteps, "kernels": "k_fwd3d_band_fast + k_back3d_col_fast"}
+        pr.set_symmetry(True)
+
     # the same pair on a dense volume (every voxel non-zero, as a
     # reconstruction iterate is): no zero-voxel shortcut applies
     dense = None
@@ -495,6 +508,7 @@ def run_b200(args):
                                        "used": bool(grouped)}},
             "parity": parity,
             "dense": dense,
+            "per_view_kernels": per_view,
             "roofline": {"bound": "issue", "kernel": kern, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
