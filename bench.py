@@ -414,7 +414,7 @@ def run_b200(args):
         per_view = {"value": 2 * VIEWS * world * psteps / (pms / 1e3), "unit": "projections/s",
                     "fwd_ms": statistics.mean(pfwd), "back_ms": statistics.mean(pback),
                     "steps": psteps, "kernels": "k_fwd3d_band_fast + k_back3d_col_fast"}
-        pr.set_symmetry(True)
+        pr.set_symmetry(True)  # back to the default group kernels
 
     # the same pair on a dense volume (every voxel non-zero, as a
     # reconstruction iterate is): no zero-voxel shortcut applies

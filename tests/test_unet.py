@@ -253,7 +253,7 @@ def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
             check(lib.trtt_b200_unet_status(_stream()), "status")
             outs.append((y.cpu(), yb.cpu()))
     finally:
-        lib.trtt_b200_conv3_set_tma(0)
+        lib.trtt_b200_conv3_set_tma(-1)
     assert torch.equal(outs[0][0], outs[1][0])
     assert torch.equal(outs[0][1], outs[1][1])
     ref = _conv_ref(torch.cat([x1, x2], 1) if c2 else x1, _bf(wt), bias.double().cpu())
@@ -282,7 +282,7 @@ def test_unet_training_step_tma_staging():
             res.append((y.cpu(), float(loss),
                         {(k, n): g.clone().cpu() for k, v in net._grads.items() for n, g in v.items()}))
     finally:
-        lib.trtt_b200_conv3_set_tma(0)
+        lib.trtt_b200_conv3_set_tma(-1)
     assert torch.equal(res[0][0], res[1][0])
     # the loss and the bias gradients are sums with float atomics: equal to
     # FP32 summation order

@@ -38,7 +38,7 @@ struct trtt_b200_plan3d {
   std::vector<View3D> hviews;
   // view groups related by turns of the grid (closed-form model, factorised
   // views): index 0 singles, 1 pairs (half turns), 2 quads (quarter turns)
-  int sym = 1;            // group kernels when they apply: 1, 2 (interleaved member profiles); 0 never
+  int sym = 2;            // group kernels when they apply: 2 (interleaved member profiles), 1; 0 never
   bool grouped = false;   // groups were found (some group has 2 or 4 views)
   int ngroups[3] = {0, 0, 0};
   DevBuf groups[3];

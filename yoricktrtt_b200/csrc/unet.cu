@@ -923,7 +923,7 @@ bool act_map(CUtensorMap *m, const void *base, int c, long rows, int box_rows)
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-int g_conv_tma = 0;  // trtt_b200_conv3_set_tma
+int g_conv_tma = -1;  // trtt_b200_conv3_set_tma; -1: TMA if the driver can encode tensor maps
 
 // Stage layout of the weight-gradient kernel: 256 rows per stage when two
 // CTAs still fit on an SM, else 128; row ranges split into chunks so that
@@ -1010,6 +1010,7 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   a.resid = resid;
   a.g = make_grid(nb, d, h, w);
   a.row0 = a.g.plane;
+  if (g_conv_tma < 0) g_conv_tma = encode_tiled() ? 1 : 0;
   if (g_conv_tma) {
     const FwdPlan pl = fwd_plan_tma(n, a.groups, a.g);
     a.rh = pl.rh;
@@ -1058,8 +1059,8 @@ int trtt_b200_conv3_set_tma(int on)
 {
   using namespace trtt;
   clear_error();
-  if (on && !encode_tiled()) return fail("conv3_set_tma: the driver provides no tensor-map encoder");
-  g_conv_tma = on ? 1 : 0;
+  if (on > 0 && !encode_tiled()) return fail("conv3_set_tma: the driver provides no tensor-map encoder");
+  g_conv_tma = on < 0 ? -1 : (on ? 1 : 0);
   return 0;
 }
 

@@ -100,9 +100,10 @@ class Projector3D:
 
     def set_symmetry(self, on=True) -> None:
         """Use (default) or bypass the group kernels that share footprints
-        between views related by turns of the volume grid; on=2 selects the
-        direct group kernel with interleaved member profiles."""
-        mode = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        between views related by turns of the volume grid: True or 2 (the
+        default: interleaved member profiles in the direct group kernel), 1
+        (one profile per member, shared-memory atomics), False or 0."""
+        mode = int(on) if not isinstance(on, bool) else (2 if on else 0)
         _lib.check(_lib.load().trtt_b200_plan3d_set_symmetry(self._h, mode),
                    "trtt_b200_plan3d_set_symmetry")
 

@@ -345,11 +345,12 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     return res
 
 
-def unet_case(size=128, batch=1, reps=1, train=1, tma=0, seed=0):
+def unet_case(size=128, batch=1, reps=1, train=1, tma=1, seed=0):
     """One U-Net case for profiling the tensor-core convolutions: ``reps``
     forward passes (and training steps when ``train``) on a batch of
     size^3 inputs; returns the CUDA-event time of the last of each.
-    ``tma=1`` stages the forward / input-gradient convolutions with TMA."""
+    ``tma=0`` stages the forward / input-gradient convolutions with
+    cp.async instead of TMA."""
     torch = _torch()
     from . import _lib
     from .unet import UNet3D
