@@ -287,6 +287,12 @@ int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *plan, int on);
  * orbit walks them). */
 int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *plan, int band_rows4, int band_rows2,
                                      int band_rows1, long back_chunk_bytes);
+/* Shape of the direct kernel for groups of 4 views: band rows (0 keeps),
+ * detector cells per u tile (0: up to 256; else 32..256) and CTAs per SM
+ * (1: up to 128 registers per thread, 2: 64; 0 keeps).  -1 if the CTA's
+ * shared memory does not fit at that occupancy. */
+int trtt_b200_plan3d_set_group_shape(trtt_b200_plan3d *plan, int band_rows4, int utile4,
+                                     int ctas_per_sm4);
 
 /* shape[0..6] = nx, ny, nz, nu, nv, nviews, number of gates. */
 int trtt_b200_plan3d_shape(const trtt_b200_plan3d *plan, long *shape);

@@ -175,3 +175,24 @@ def test_group_batch_entry_point(oracle_port, case, job):
     assert np.isfinite(out).all() and rel_l2(out, ref) <= TOL
     call(out, 1)
     assert rel_l2(out, 2 * ref) <= TOL
+
+
+def test_group_quad_shapes(oracle_port):
+    """Other shapes of the quad direct kernel (band rows, cells per u tile,
+    CTAs per SM with their register budget) give the same projection."""
+    import torch
+    from yoricktrtt_b200.projectors import Projector3D
+    sc = _scan(views=8, nu=100, nv=60, us=0.6)
+    pr = Projector3D(sc)
+    vol = torch.tensor(P.ellipsoids_3d(24, 24, 16, n=6, seed=9), device="cuda")
+    ref = pr.forward(vol).double().cpu().numpy()
+    for shape in [(16, 32, 2), (32, 64, 1), (8, 0, 2), (60, 50, 1)]:
+        pr.set_group_shape(*shape)
+        got = pr.forward(vol).double().cpu().numpy()
+        pr.status()
+        assert rel_l2(got, ref) <= 1e-6, shape
+    vol64 = np.ascontiguousarray(vol.double().cpu().numpy())
+    for v in (0, 3, 7):
+        r = np.zeros((sc.nv, sc.nu))
+        oracle_port.cb3d(r, vol64, sc, v, 0)
+        assert rel_l2(got[v], r) <= TOL

@@ -62,6 +62,7 @@ SIGNATURES = {
     "trtt_b200_plan3d_set_persistent": (_I, [_vp, _I, _I, _D, _I]),
     "trtt_b200_plan3d_set_symmetry": (_I, [_vp, _I]),
     "trtt_b200_plan3d_set_group_tiles": (_I, [_vp, _I, _I, _I, _L]),
+    "trtt_b200_plan3d_set_group_shape": (_I, [_vp, _I, _I, _I]),
     "trtt_b200_plan3d_destroy": (_I, [_vp]),
     "trtt_b200_plan2d_create": (_I, [C.POINTER(_vp), _I, _L, _L, _D, _I, _dp, _L, _D, _dp, _L,
                                       _D, _L, _dp, _dp]),

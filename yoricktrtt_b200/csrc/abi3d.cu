@@ -43,6 +43,7 @@ struct trtt_b200_plan3d {
   int ngroups[3] = {0, 0, 0};
   DevBuf groups[3];
   int gband[3] = {64, 32, 32};  // direct: band rows per group size
+  int gutile4 = 0, gminb4 = 1;  // direct, quads: cells per u tile (0: up to 256), CTAs per SM
   long back_chunk_bytes = 32L << 20;  // transpose: detector bytes per launch
   // persistent weighted least-squares launch
   int wls_rows = 32, wls_ctas = 1, wls_extra = 0;
@@ -350,6 +351,28 @@ extern "C" int trtt_b200_plan3d_wls_grad(trtt_b200_plan3d *pl, const float *vol,
   return 0;
 }
 
+extern "C" int trtt_b200_plan3d_set_group_shape(trtt_b200_plan3d *pl, int band_rows4, int utile4,
+                                                int ctas_per_sm4)
+{
+  clear_error();
+  if (!pl) return fail("plan3d_set_group_shape: null plan");
+  if (band_rows4 < 0 || band_rows4 == 1) return fail("plan3d_set_group_shape: band rows must be 0 (keep) or >= 2");
+  if (utile4 < 0 || utile4 > 256 || (utile4 > 0 && utile4 < 32))
+    return fail("plan3d_set_group_shape: u tile must be 0 (automatic) or in [32, 256]");
+  if (ctas_per_sm4 < 0 || ctas_per_sm4 > 2) return fail("plan3d_set_group_shape: CTAs per SM must be 0, 1 or 2");
+  const int rows = std::min(band_rows4 ? band_rows4 : pl->gband[2], pl->P.nv);
+  const int umax = utile4 > 0 ? utile4 : 256;
+  const int usplit = (pl->P.nu + umax - 1) / umax, ut = (pl->P.nu + usplit - 1) / usplit;
+  const int cpsm = ctas_per_sm4 ? ctas_per_sm4 : pl->gminb4;
+  const size_t smem = group_fwd_smem(4, rows, ut, 16);
+  if (smem > (cpsm == 2 ? 113u : 227u) * 1024u)
+    return fail("plan3d_set_group_shape: the quad band does not fit in shared memory at that occupancy");
+  if (band_rows4) pl->gband[2] = band_rows4;
+  pl->gutile4 = utile4;
+  if (ctas_per_sm4) pl->gminb4 = ctas_per_sm4;
+  return 0;
+}
+
 extern "C" int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *pl)
 {
   return pl && pl->factorized ? 1 : 0;
@@ -408,10 +431,12 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
       L.sino = dst;
       L.sino_view_stride = npix;
       L.band_rows = std::min(pl->gband[q], P.nv);
-      L.usplit = (P.nu + 255) / 256;
+      const int umax = (G == 4 && pl->gutile4 > 0) ? pl->gutile4 : 256;
+      L.usplit = (P.nu + umax - 1) / umax;
       L.utile = (P.nu + L.usplit - 1) / L.usplit;
       L.warps = 16;
       L.interleave = pl->sym == 2 ? 1 : 0;
+      L.minb = G == 4 ? pl->gminb4 : 2;
       L.err = pl->err.as<int>();
       TRTT_CK(launch_fwd3d_group(L, G, st));
       count_launch();

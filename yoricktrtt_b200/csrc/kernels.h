@@ -69,6 +69,7 @@ struct GroupFwdLaunch {
   int usplit, utile;     // u tiles per band and cells per tile (utile <= 256)
   int warps;
   int interleave = 0;    // 1: member profiles interleaved per cell, plain updates where they apply
+  int minb = 1;          // groups of 4: 1 (128 registers per thread) or 2 CTAs per SM (64)
   int *err;
 };
 

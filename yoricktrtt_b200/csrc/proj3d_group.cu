@@ -106,26 +106,27 @@ __device__ __forceinline__ void column_k_range(const ColGeo<MODEL_CUBIC> &c, dou
   khi = (int)kb;
 }
 
-// Add a[0..G) into the G interleaved member slots of one profile cell.
+// cell[m] += w * xr[m] for the G interleaved member slots of one profile
+// cell (one vector load, G fused multiply-adds, one vector store).
 template <int G>
-__device__ __forceinline__ void cell_add(float *cell, const float (&a)[G])
+__device__ __forceinline__ void cell_fma(float *cell, float w, const float (&xr)[G])
 {
   if constexpr (G == 4) {
     float4 *q = reinterpret_cast<float4 *>(cell);
     float4 v = *q;
-    v.x += a[0];
-    v.y += a[1];
-    v.z += a[2];
-    v.w += a[3];
+    v.x = fmaf(w, xr[0], v.x);
+    v.y = fmaf(w, xr[1], v.y);
+    v.z = fmaf(w, xr[2], v.z);
+    v.w = fmaf(w, xr[3], v.w);
     *q = v;
   } else if constexpr (G == 2) {
     float2 *q = reinterpret_cast<float2 *>(cell);
     float2 v = *q;
-    v.x += a[0];
-    v.y += a[1];
+    v.x = fmaf(w, xr[0], v.x);
+    v.y = fmaf(w, xr[1], v.y);
     *q = v;
   } else {
-    *cell += a[0];
+    *cell = fmaf(w, xr[0], *cell);
   }
 }
 
@@ -155,8 +156,8 @@ __device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D 
 // ---------------------------------------------------------------------------
 // Direct projector over view groups
 // ---------------------------------------------------------------------------
-template <int GEOM, int G, bool IL>
-__global__ void __launch_bounds__(512, (G == 4 ? 1 : 2))
+template <int GEOM, int G, bool IL, int MINB>
+__global__ void __launch_bounds__(512, MINB)
 k_fwd3d_group(const GroupFwdLaunch A)
 {
   extern __shared__ float sm[];
@@ -271,27 +272,21 @@ k_fwd3d_group(const GroupFwdLaunch A)
           if (Lw <= 0) continue;
           const float2 start = make_float2(fmaf((float)(f0 - up.lo0), up.inc.x, up.start.x),
                                            fmaf((float)(f1 - up.lo1), up.inc.y, up.start.y));
-          float2 xr[G];
+          float xr0[G], xr1[G];
 #pragma unroll
-          for (int m = 0; m < G; ++m) xr[m] = mul2(x[m], up.rho);
+          for (int m = 0; m < G; ++m) {
+            const float2 t = mul2(x[m], up.rho);
+            xr0[m] = t.x;
+            xr1[m] = t.y;
+          }
           float2 Fp = f2(0.0f);
           float2 lf = f2(1.0f);
           for (int l = 0; l < Lw; ++l) {
             const float2 F = cubic_prim2(fma2(lf, up.inc, start));
             const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
             const int c0 = f0 + l, c1 = f1 + l;
-            if (l < L0 && c0 >= u0) {
-              float a[G];
-#pragma unroll
-              for (int m = 0; m < G; ++m) a[m] = w.x * xr[m].x;
-              cell_add<G>(prof + (c0 - u0) * G, a);
-            }
-            if (l < L1 && c1 >= u0) {
-              float a[G];
-#pragma unroll
-              for (int m = 0; m < G; ++m) a[m] = w.y * xr[m].y;
-              cell_add<G>(prof + (c1 - u0) * G, a);
-            }
+            if (l < L0 && c0 >= u0) cell_fma<G>(prof + (c0 - u0) * G, w.x, xr0);
+            if (l < L1 && c1 >= u0) cell_fma<G>(prof + (c1 - u0) * G, w.y, xr1);
             __syncwarp();
             Fp = F;
             lf = add2(lf, f2(1.0f));
@@ -685,7 +680,11 @@ cudaError_t fwd_group(const GroupFwdLaunch &L, cudaStream_t st)
   const int nbands = (L.P.nv + L.band_rows - 1) / L.band_rows;
   dim3 grid(nbands * L.usplit, L.ngroups);
   const size_t smem = group_fwd_smem(G, L.band_rows, L.utile, L.warps);
-  auto kern = L.interleave ? k_fwd3d_group<GEOM, G, true> : k_fwd3d_group<GEOM, G, false>;
+  // register budget: 128 per thread (one 16-warp CTA per SM) or 64 (two);
+  // groups of 1 and 2 views always fit two CTAs
+  auto kern = (G == 4 && L.minb == 1)
+                  ? (L.interleave ? k_fwd3d_group<GEOM, G, true, 1> : k_fwd3d_group<GEOM, G, false, 1>)
+                  : (L.interleave ? k_fwd3d_group<GEOM, G, true, 2> : k_fwd3d_group<GEOM, G, false, 2>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<grid, L.warps * 32, smem, st>>>(L);

@@ -113,6 +113,12 @@ class Projector3D:
         _lib.check(_lib.load().trtt_b200_plan3d_groups(self._h, c), "trtt_b200_plan3d_groups")
         return tuple(int(x) for x in c)
 
+    def set_group_shape(self, band_rows4=0, utile4=0, ctas_per_sm4=0):
+        """Direct kernel shape for groups of 4 views (see
+        trtt_b200_plan3d_set_group_shape)."""
+        _lib.check(_lib.load().trtt_b200_plan3d_set_group_shape(self._h, band_rows4, utile4, ctas_per_sm4),
+                   "trtt_b200_plan3d_set_group_shape")
+
     def set_group_tiles(self, band_rows4=0, band_rows2=0, band_rows1=0, back_chunk_bytes=0):
         _lib.check(_lib.load().trtt_b200_plan3d_set_group_tiles(
             self._h, band_rows4, band_rows2, band_rows1, back_chunk_bytes),

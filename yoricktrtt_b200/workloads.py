@@ -300,14 +300,15 @@ def learned_eval(weights=None, n_test=20, eval_maxiter=500, ref_maxiter=600, see
 
 
 def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps=1, dense=0,
-                   tiles=None, sym=1, seed=0):
+                   tiles=None, sym=2, gshape=None, seed=0):
     """One cone-beam projector case for profiling: an n x n x nz volume of 20
     ellipsoids (``dense=1`` adds a positive floor so that every voxel is
     non-zero), ``views`` views on an nd x nd detector, SID 1000 mm, SDD
     1500 mm, closed-form cubic footprint, columns layout.  Runs ``reps``
     direct and/or transpose launches, checks the status flag and returns the
     CUDA-event time of the last launch of each direction.  ``tiles`` is a
-    set_tiles() argument list; ``sym=0`` bypasses the group kernels."""
+    set_tiles() argument list; ``sym=0`` bypasses the group kernels, ``sym=1``
+    selects per-member profiles; ``gshape`` is a set_group_shape() list."""
     torch = _torch()
     from . import geometry as G, phantoms as P
     from .projectors import Projector3D, columns_from_xyz
@@ -320,11 +321,13 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     if tiles:
         pr.set_tiles(*tiles)
     pr.set_symmetry(int(sym))
+    if gshape:
+        pr.set_group_shape(*gshape)
     x = columns_from_xyz(torch.tensor(vol, device="cuda"))
     y = torch.zeros(pr.detector_shape(), device="cuda")
     b = torch.zeros_like(x)
     res = {"config": f"cone {n}x{n}x{nz} -> {views} x {nd}^2, cubic, {'dense' if dense else 'phantom'}",
-           "groups": pr.groups(), "symmetry": int(sym)}
+           "groups": pr.groups(), "symmetry": int(sym), "gshape": gshape}
     for _ in range(reps):
         if direct:
             a, e = _events()
