@@ -273,7 +273,8 @@ extern "C" int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *pl, int band_r
     if (req[q] == 0) continue;
     if (req[q] < 2) return fail("plan3d_set_group_tiles: band rows must be >= 2");
     const int r = std::min(req[q], pl->P.nv);
-    if (group_fwd_smem(group_size_of(q), r, utile, 16) > 227u * 1024u)
+    const int G = group_size_of(q), minb = G == 4 ? pl->gminb4 : 2;
+    if (group_fwd_smem(G, r, utile, group_fwd_warps(G, r, utile, minb)) > 227u * 1024u)
       return fail("plan3d_set_group_tiles: band does not fit in shared memory");
   }
   for (int q = 0; q < 3; ++q)
@@ -364,7 +365,7 @@ extern "C" int trtt_b200_plan3d_set_group_shape(trtt_b200_plan3d *pl, int band_r
   const int umax = utile4 > 0 ? utile4 : 256;
   const int usplit = (pl->P.nu + umax - 1) / umax, ut = (pl->P.nu + usplit - 1) / usplit;
   const int cpsm = ctas_per_sm4 ? ctas_per_sm4 : pl->gminb4;
-  const size_t smem = group_fwd_smem(4, rows, ut, 16);
+  const size_t smem = group_fwd_smem(4, rows, ut, group_fwd_warps(4, rows, ut, cpsm));
   if (smem > (cpsm == 2 ? 113u : 227u) * 1024u)
     return fail("plan3d_set_group_shape: the quad band does not fit in shared memory at that occupancy");
   if (band_rows4) pl->gband[2] = band_rows4;
@@ -434,9 +435,9 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
       const int umax = (G == 4 && pl->gutile4 > 0) ? pl->gutile4 : 256;
       L.usplit = (P.nu + umax - 1) / umax;
       L.utile = (P.nu + L.usplit - 1) / L.usplit;
-      L.warps = 16;
       L.interleave = pl->sym == 2 ? 1 : 0;
       L.minb = G == 4 ? pl->gminb4 : 2;
+      L.warps = group_fwd_warps(G, L.band_rows, L.utile, L.minb);
       L.err = pl->err.as<int>();
       TRTT_CK(launch_fwd3d_group(L, G, st));
       count_launch();
@@ -662,7 +663,9 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
       L.band_rows = (int)std::min<long>(G == 1 ? 64 : 32, nv);
       L.usplit = usplit;
       L.utile = utile;
-      L.warps = 16;
+      L.interleave = 1;
+      L.minb = G == 4 ? 1 : 2;
+      L.warps = group_fwd_warps(G, L.band_rows, utile, L.minb);
       L.err = D.err.as<int>();
       const long bands = (nv + L.band_rows - 1) / L.band_rows;
       const long per_wave = (long)D.sms * (G == 4 ? 1 : 2);

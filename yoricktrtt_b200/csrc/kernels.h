@@ -69,7 +69,7 @@ struct GroupFwdLaunch {
   int usplit, utile;     // u tiles per band and cells per tile (utile <= 256)
   int warps;
   int interleave = 0;    // 1: member profiles interleaved per cell, plain updates where they apply
-  int minb = 1;          // groups of 4: 1 (128 registers per thread) or 2 CTAs per SM (64)
+  int minb = 1;          // groups of 4: 1 CTA per SM (up to 22 warps) or 2 (64 registers per thread)
   int *err;
 };
 
@@ -119,6 +119,7 @@ int wls_kp(int nz);
 cudaError_t launch_wls_persistent(WlsLaunch L, int sms, cudaStream_t st);
 
 size_t group_fwd_smem(int G, int band_rows, int utile, int warps);
+int group_fwd_warps(int G, int band_rows, int utile, int minb);
 int group_orbits(int G, int nx, int ny);
 cudaError_t launch_fwd3d_group(const GroupFwdLaunch &L, int G, cudaStream_t st);
 cudaError_t launch_back3d_group(const GroupBackLaunch &L, int G, cudaStream_t st);

@@ -106,6 +106,26 @@ __device__ __forceinline__ void column_k_range(const ColGeo<MODEL_CUBIC> &c, dou
   khi = (int)kb;
 }
 
+// The G member values of one interleaved profile or band cell.
+template <int G> struct VecOf;
+template <> struct VecOf<4> { using T = float4; };
+template <> struct VecOf<2> { using T = float2; };
+template <> struct VecOf<1> { using T = float; };
+
+__device__ __forceinline__ void vec_fma(float4 &b, float w, const float4 &p)
+{
+  b.x = fmaf(w, p.x, b.x);
+  b.y = fmaf(w, p.y, b.y);
+  b.z = fmaf(w, p.z, b.z);
+  b.w = fmaf(w, p.w, b.w);
+}
+__device__ __forceinline__ void vec_fma(float2 &b, float w, const float2 &p)
+{
+  b.x = fmaf(w, p.x, b.x);
+  b.y = fmaf(w, p.y, b.y);
+}
+__device__ __forceinline__ void vec_fma(float &b, float w, const float &p) { b = fmaf(w, p, b); }
+
 // cell[m] += w * xr[m] for the G interleaved member slots of one profile
 // cell (one vector load, G fused multiply-adds, one vector store).
 template <int G>
@@ -151,16 +171,59 @@ __device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D 
   }
 }
 
+__device__ __forceinline__ unsigned long long timer_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Exclusive use of one band row by a warp (lane 0 takes the lock, the warp
+// then updates the row with plain loads and stores).  The wait is bounded:
+// past 2 s the warp sets TRTT_ERR_STALL and skips the row.  A holder
+// releases after a few hundred cycles, so the limit is never reached in a
+// correct run.
+__device__ __forceinline__ bool row_lock(int *lock, int *err)
+{
+  int got = 1;
+  if ((threadIdx.x & 31) == 0) {
+    if (atomicCAS(lock, 0, 1) != 0) {
+      const unsigned long long t0 = timer_ns();
+      while (atomicCAS(lock, 0, 1) != 0) {
+        if (timer_ns() - t0 > 2000000000ull) {
+          atomicOr(err, TRTT_ERR_STALL);
+          got = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence_block();
+  }
+  got = __shfl_sync(FULLM, got, 0);
+  __syncwarp();
+  return got != 0;
+}
+
+__device__ __forceinline__ void row_unlock(int *lock)
+{
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence_block();
+    atomicExch(lock, 0);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Direct projector over view groups
 // ---------------------------------------------------------------------------
 template <int GEOM, int G, bool IL, int MINB>
-__global__ void __launch_bounds__(512, MINB)
+__global__ void __launch_bounds__(MINB == 1 ? 704 : 512, MINB)
 k_fwd3d_group(const GroupFwdLaunch A)
 {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   __shared__ View3D sV;
   __shared__ int s_next;
   __shared__ int s_mem[4];
@@ -173,9 +236,11 @@ k_fwd3d_group(const GroupFwdLaunch A)
   const int v0 = band * R, v1 = min(v0 + R, nv);
   const int u0 = ut * U, u1 = min(u0 + U, nu);
   const int grp = blockIdx.y;
-  float *bands = sm;                                    // [G][R][U]
-  float *prof = sm + G * R * U + warp * G * U;          // [G][U], this warp
+  // member bands: [G][R][U], or [R][U][G] with interleaved profiles (IL)
+  float *bands = sm;
+  float *prof = sm + G * R * U + warp * G * U;          // [G][U] or [U][G], this warp
   float *wv = sm + G * R * U + nwarps * G * U + warp * R;  // [R], this warp
+  int *row_locks = reinterpret_cast<int *>(sm + G * R * U + nwarps * G * U + nwarps * R);  // [R]
   const int base = A.groups[4 * grp];
   if (threadIdx.x < (int)(sizeof(View3D) / 8))
     reinterpret_cast<double *>(&sV)[threadIdx.x] =
@@ -183,6 +248,7 @@ k_fwd3d_group(const GroupFwdLaunch A)
   if (threadIdx.x < 4) s_mem[threadIdx.x] = A.groups[4 * grp + threadIdx.x];
   if (threadIdx.x == 0) s_next = 0;
   for (int t = threadIdx.x; t < G * R * U; t += blockDim.x) bands[t] = 0.f;
+  for (int t = threadIdx.x; t < R; t += blockDim.x) row_locks[t] = 0;
   for (int t = lane; t < G * U; t += 32) prof[t] = 0.f;
   __syncthreads();
   const View3D &V = sV;
@@ -363,54 +429,65 @@ k_fwd3d_group(const GroupFwdLaunch A)
       hi = __reduce_max_sync(FULLM, hi);
       __syncwarp();
       if (lo < hi) {
-        // spread: band_m[r][u] += wv[r] * P_m[u]; each profile read once
-        // into registers (and cleared), one shared atomic per cell and row
         constexpr int CH = 8;  // U <= 256 cells per tile
-        float pvs[G][CH];
         if constexpr (IL) {
+          // spread: band[r][u][m] += wv[r] * P[u][m].  The warp takes each
+          // of its rows exclusively (row lock) and updates the G members of
+          // a cell with one vector load and store; the profile is read once
+          // into registers and cleared.
+          using VecG = typename VecOf<G>::T;
+          VecG pv[CH];
 #pragma unroll
           for (int q = 0; q < CH; ++q) {
             const int u = lo + lane + 32 * q;
-            float a[G];
-#pragma unroll
-            for (int m = 0; m < G; ++m) a[m] = 0.f;
+            pv[q] = VecG{};
             if (u < hi) {
-              float *cell = prof + (u - u0) * G;
+              VecG *cell = reinterpret_cast<VecG *>(prof + (u - u0) * G);
+              pv[q] = *cell;
+              *cell = VecG{};
+            }
+          }
+          for (int r = 0; r < nr; ++r) {
+            const float w = wv[r];
+            const int row = rb - v0 + r;
+            if (!row_lock(row_locks + row, A.err)) continue;
+            VecG *brow = reinterpret_cast<VecG *>(bands + (size_t)row * U * G);
 #pragma unroll
-              for (int m = 0; m < G; ++m) {
-                a[m] = cell[m];
-                cell[m] = 0.f;
+            for (int q = 0; q < CH; ++q) {
+              const int u = lo + lane + 32 * q;
+              if (u < hi) {
+                VecG b = brow[u - u0];
+                vec_fma(b, w, pv[q]);
+                brow[u - u0] = b;
               }
             }
-#pragma unroll
-            for (int m = 0; m < G; ++m) pvs[m][q] = a[m];
+            row_unlock(row_locks + row);
           }
-        }
+        } else {
+          // spread: band_m[r][u] += wv[r] * P_m[u]; each profile read once
+          // into registers (and cleared), one shared atomic per cell and row
 #pragma unroll
-        for (int m = 0; m < G; ++m) {
-          float pv[CH];
-          float *pm = prof + m * U;
+          for (int m = 0; m < G; ++m) {
+            float pv[CH];
+            float *pm = prof + m * U;
 #pragma unroll
-          for (int q = 0; q < CH; ++q) {
-            const int u = lo + lane + 32 * q;
-            if constexpr (IL) {
-              pv[q] = pvs[m][q];
-            } else {
+            for (int q = 0; q < CH; ++q) {
+              const int u = lo + lane + 32 * q;
               pv[q] = 0.f;
               if (u < hi) {
                 pv[q] = pm[u - u0];
                 pm[u - u0] = 0.f;
               }
             }
-          }
-          float *bm = bands + (m * R + (rb - v0)) * U;
-          for (int r = 0; r < nr; ++r) {
-            const float w = wv[r];
-            float *row = bm + r * U;
+            float *bm = bands + (m * R + (rb - v0)) * U;
+            for (int r = 0; r < nr; ++r) {
+              const float w = wv[r];
+              float *row = bm + r * U;
 #pragma unroll
-            for (int q = 0; q < CH; ++q) {
-              const int u = lo + lane + 32 * q;
-              if (u < hi) atomicAdd(row + (u - u0), w * pv[q]);
+              for (int q = 0; q < CH; ++q) {
+                const int u = lo + lane + 32 * q;
+                if (u < hi) atomicAdd(row + (u - u0), w * pv[q]);
+              }
             }
           }
         }
@@ -423,10 +500,9 @@ k_fwd3d_group(const GroupFwdLaunch A)
 #pragma unroll
   for (int m = 0; m < G; ++m) {
     float *out = A.sino + (long)s_mem[m] * A.sino_view_stride;
-    const float *bm = bands + m * R * U;
     for (int t = threadIdx.x; t < nrow * ncell; t += blockDim.x) {
       const int r = t / ncell, u = t - r * ncell;
-      out[(long)(v0 + r) * nu + u0 + u] += bm[r * U + u];
+      out[(long)(v0 + r) * nu + u0 + u] += IL ? bands[(r * U + u) * G + m] : bands[(m * R + r) * U + u];
     }
   }
 }
@@ -711,8 +787,17 @@ cudaError_t back_group(const GroupBackLaunch &L, cudaStream_t st)
 
 size_t group_fwd_smem(int G, int band_rows, int utile, int warps)
 {
+  // bands, one profile and one row-weight list per warp, one lock per row
   return sizeof(float) * ((size_t)G * band_rows * utile + (size_t)warps * G * utile +
-                          (size_t)warps * band_rows);
+                          (size_t)warps * band_rows + (size_t)band_rows);
+}
+
+int group_fwd_warps(int G, int band_rows, int utile, int minb)
+{
+  // quads at one CTA per SM: 22 warps (up to 93 registers each) where the
+  // bands and 22 profiles fit in shared memory, else 16
+  if (G == 4 && minb == 1 && group_fwd_smem(4, band_rows, utile, 22) + 1024 <= 227u * 1024u) return 22;
+  return 16;
 }
 
 int group_orbits(int G, int nx, int ny)
