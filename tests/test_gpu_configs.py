@@ -126,6 +126,21 @@ def test_c3_cubic_dense(oracle_port, c3):
     assert worst <= TOL
 
 
+def test_c3_cubic_per_view_kernels(oracle_port, c3):
+    """The per-view band and column kernels (view groups off) at the same
+    size: long voxel columns select the row-locked spread."""
+    from yoricktrtt_b200.projectors import Projector3D
+    sc, vol = c3
+    pr = Projector3D(sc)
+    pr.set_symmetry(0)
+    worst, errs = _check_forward(oracle_port, sc, vol, _forward_views(pr, vol, C3_SAMPLE[1::2]))
+    print(f"C3 per-view kernels forward rel-L2 per view: {['%.2e' % e for e in errs]}")
+    assert worst <= TOL
+    err_b = _check_transpose(oracle_port, sc, pr, C3_SAMPLE[1::2])
+    print(f"C3 per-view kernels transpose rel-L2: {err_b:.2e}")
+    assert err_b <= TOL
+
+
 def test_c3_table(oracle_port, c3):
     from yoricktrtt_b200.projectors import Projector3D
     sc, vol = c3

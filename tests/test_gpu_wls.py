@@ -107,6 +107,18 @@ def test_wls_small_gated(oracle_port, weighted):
     assert abs(cost - cost2) <= 1e-6 * abs(cost2) and rel_l2(grad, grad2) <= 1e-6
 
 
+def test_wls_long_columns(oracle_port):
+    """Columns of 128 voxels: the band items spread under row locks."""
+    nt = 2
+    sc, t_index = _gated_scan(nt, [4, 3], n=(16, 12, 128), nd=200, rsc=150.0, rsd=225.0, seed=4)
+    gates = P.breathing_gates(16, 12, 128, nt, 1.0, amplitude_mm=4.0, seed=5)
+    (cost, grad, y, w), (cost2, grad2), _, _ = _run(sc, t_index, nt, gates, True)
+    ref_cost, ref_grad = _oracle_wls(oracle_port, sc, t_index, nt, gates, y, w)
+    assert abs(cost - ref_cost) <= TOL * abs(ref_cost)
+    assert rel_l2(grad, ref_grad) <= TOL
+    assert abs(cost - cost2) <= 1e-6 * abs(cost2) and rel_l2(grad, grad2) <= 1e-6
+
+
 def test_wls_config4_autotuned(oracle_port):
     """10 gates of 128x128x64, views per gate drawn from U{20..60}, 256^2."""
     nt = 10

@@ -223,7 +223,7 @@ extern "C" int trtt_b200_plan3d_set_tiles(trtt_b200_plan3d *pl, int band_rows, i
   if (band_rows < 0) {
     pl->band_rows = 0;
   } else if (band_rows > 0) {
-    const long smem = 4L * ((long)band_rows * pl->P.nu + (long)pl->warps * pl->P.nu + (long)pl->warps * band_rows);
+    const long smem = (long)band_fast_smem(pl->P.nu, band_rows, pl->warps);
     if (smem > 227L * 1024) return fail("plan3d_set_tiles: band does not fit in shared memory");
     pl->band_rows = band_rows > pl->P.nv ? pl->P.nv : band_rows;
   }

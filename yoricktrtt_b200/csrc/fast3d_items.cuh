@@ -5,8 +5,8 @@
 //  * band item (direct): one CTA accumulates, for one view, the detector
 //    rows [v0, v1) in shared memory: warps pull 32-column chunks from a
 //    shared counter, build each hit column's u-profile (two voxels per lane,
-//    packed FP32x2) with shared-memory atomics and spread it over the band
-//    rows with the column's v-weights;
+//    packed FP32x2) and spread it over the band rows with the column's
+//    v-weights, one row at a time under a row lock;
 //  * column item (transpose): one warp gathers, for one voxel column and
 //    k range, the contributions of every (view, weight) entry of a gate: per
 //    view the v-collapsed profile Q[u] = sum_v w(v) pix[v][u] is built in
@@ -23,15 +23,94 @@ namespace trtt {
 
 static constexpr int SPREAD_CHUNKS = 16;  // footprints up to 512 cells wide spread from registers
 
+// True when floor(uc_k - hs_k), the first cell of voxel k's u-footprint
+// before any clamp, strictly increases or decreases along the column: the
+// voxels of one warp step then write distinct cells at every footprint
+// offset l, so a warp can update its profile with plain loads and stores.
+// |d uc/dk| = |B|; hs = hs0 h_u0 magn delta_u varies by at most
+// hs0 h_u0m |B| max|uc - a12| u_scl^2 inv_den per voxel.
+template <int GEOM>
+__device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D &V,
+                                                const ColGeo<MODEL_CUBIC> &c)
+{
+  const double b = fabs(c.B);
+  if constexpr (GEOM == GEOM_CONE) {
+    const double ua = c.A, ub = fma(c.B, (double)(P.nz - 1), c.A);
+    const double um = fmax(fabs(ua - V.a12), fabs(ub - V.a12));
+    const double dhs = P.hs0 * (double)c.h_u0m * b * um * P.u_scl * P.u_scl * (double)c.inv_den;
+    return b - dhs >= 1.002;
+  } else {
+    return b >= 1.002;
+  }
+}
+
+__device__ __forceinline__ unsigned long long timer_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Exclusive use of one band row by a warp (lane 0 takes the lock, the warp
+// then updates the row with plain loads and stores).  The wait is bounded:
+// past 2 s the warp sets TRTT_ERR_STALL and skips the row.  A holder
+// releases after a few hundred cycles, so the limit is never reached in a
+// correct run.
+__device__ __forceinline__ bool row_lock(int *lock, int *err)
+{
+  int got = 1;
+  if ((threadIdx.x & 31) == 0) {
+    if (atomicCAS(lock, 0, 1) != 0) {
+      const unsigned long long t0 = timer_ns();
+      while (atomicCAS(lock, 0, 1) != 0) {
+        if (timer_ns() - t0 > 2000000000ull) {
+          atomicOr(err, TRTT_ERR_STALL);
+          got = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence_block();
+  }
+  got = __shfl_sync(FULLM, got, 0);
+  __syncwarp();
+  return got != 0;
+}
+
+__device__ __forceinline__ void row_unlock(int *lock)
+{
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence_block();
+    atomicExch(lock, 0);
+  }
+}
+
+
 // Band item.  acc: band_rows x nu floats (zeroed by the caller), prof: this
 // warp's nu-float profile (zero on entry and on exit), wv: this warp's
-// band_rows floats, s_next: the CTA's chunk counter (0 on entry).  All
-// threads of the CTA call it; it returns without a final barrier.
+// band_rows floats, locks: band_rows ints (zero, shared by the CTA), s_next:
+// the CTA's chunk counter (0 on entry), lock_spread: spread mode (below,
+// the same for the whole CTA).  All threads of the CTA call it; it returns
+// without a final barrier.
+//
+// Profile: where floor(uc - hs) is strictly monotone along the column
+// (column_monotone) the 64 voxels of a warp step write 64 distinct cells at
+// every footprint offset, so each voxel walks its footprint from the
+// unclamped first cell (primitive 0 there) with plain loads and stores,
+// steps ordered by __syncwarp; other columns use shared atomics.  Spread:
+// with lock_spread the warp takes each band row exclusively (row_lock) and
+// adds w(v) P[u] with plain loads and stores, else one shared atomic per
+// cell and row.  Shared float atomics are compare-and-swap loops, so the
+// locks pay on long rows (long voxel columns); on short ones the warps
+// meet on the same rows and the atomics are faster (band_lock_spread).
 template <int GEOM>
 __device__ __forceinline__ void band_item(const Params3D &P, const View3D &V,
                                           const float *__restrict__ vol, long gate_stride, int v0,
                                           int v1, int band_rows, float *acc, float *prof, float *wv,
-                                          int *s_next, int *__restrict__ err)
+                                          int *locks, int *s_next, int *__restrict__ err,
+                                          bool lock_spread)
 {
   const int lane = threadIdx.x & 31;
   const int nu = P.nu, nz = P.nz;
@@ -61,43 +140,92 @@ __device__ __forceinline__ void band_item(const Params3D &P, const View3D &V,
       for (int r = lane; r < nr; r += 32) wv[r] = axis_weight<MODEL_CUBIC>(cc.vax, rb - vl + r, P);
       int lo = INT_MAX, hi = INT_MIN;
       const long cbase = (long)col * nz;
-      for (int k0 = lane; k0 < nz; k0 += 64) {
-        const int k1 = k0 + 32;
-        const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
-        const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
-        if (x0 == 0.0f && x1 == 0.0f) continue;
-        UPair up;
-        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
-        if (x0 == 0.0f) up.n0 = 0;
-        if (x1 == 0.0f) up.n1 = 0;
-        const int L = max(up.n0, up.n1);
-        if (L <= 0) continue;
-        const float2 xr = mul2(make_float2(x0, x1), up.rho);
-        float2 Fp = first_edge_prim2(up);
-        float2 lf = f2(1.0f);
-        for (int l = 0; l < L; ++l) {
-          const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
-          const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
-          if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
-          if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
-          Fp = F;
-          lf = add2(lf, f2(1.0f));
+      if (column_monotone<GEOM>(P, V, cc)) {
+        for (int kb = 0; kb < nz; kb += 64) {
+          const int k0 = kb + lane, k1 = k0 + 32;
+          const float x0 = (k0 < nz) ? vox_val(vol, gate_stride, V, cbase + k0) : 0.0f;
+          const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+          if (!__any_sync(FULLM, x0 != 0.0f || x1 != 0.0f)) continue;
+          UPair up;
+          voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+          if (x0 == 0.0f) up.n0 = 0;
+          if (x1 == 0.0f) up.n1 = 0;
+          const double uc0 = fma(cc.B, (double)k0, cc.A), uc1 = fma(cc.B, (double)k1, cc.A);
+          const float2 hsv = mul2(make_float2(__frcp_rn(up.inc.x), __frcp_rn(up.inc.y)),
+                                  f2((float)P.hs0));
+          const int f0 = __double2int_rd(uc0 - (double)hsv.x), f1 = __double2int_rd(uc1 - (double)hsv.y);
+          // the reference's first cell is f clamped to [0, nu-1]: cells left
+          // of the detector are not written; a footprint that starts past it
+          // (f >= nu) gives its one clamped cell weight 0 - 0 and is dropped
+          const int e0 = up.n0 > 0 ? up.lo0 + up.n0 : INT_MIN;
+          const int e1 = up.n1 > 0 ? up.lo1 + up.n1 : INT_MIN;
+          const int L0 = (up.n0 > 0 && f0 < nu) ? max(e0 - f0, 0) : 0;
+          const int L1 = (up.n1 > 0 && f1 < nu) ? max(e1 - f1, 0) : 0;
+          const int Lw = __reduce_max_sync(FULLM, max(max(L0, L1), 0));
+          if (Lw <= 0) continue;
+          const float2 start = make_float2(fmaf((float)(f0 - up.lo0), up.inc.x, up.start.x),
+                                           fmaf((float)(f1 - up.lo1), up.inc.y, up.start.y));
+          const float2 xr = mul2(make_float2(x0, x1), up.rho);
+          float2 Fp = f2(0.0f);
+          float2 lf = f2(1.0f);
+          for (int l = 0; l < Lw; ++l) {
+            const float2 F = cubic_prim2(fma2(lf, up.inc, start));
+            const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+            const int c0 = f0 + l, c1 = f1 + l;
+            if (l < L0 && c0 >= 0) prof[c0] = fmaf(w.x, xr.x, prof[c0]);
+            if (l < L1 && c1 >= 0) prof[c1] = fmaf(w.y, xr.y, prof[c1]);
+            __syncwarp();
+            Fp = F;
+            lf = add2(lf, f2(1.0f));
+          }
+          if (L0 > 0 && e0 > max(f0, 0)) {
+            lo = min(lo, max(f0, 0));
+            hi = max(hi, e0);
+          }
+          if (L1 > 0 && e1 > max(f1, 0)) {
+            lo = min(lo, max(f1, 0));
+            hi = max(hi, e1);
+          }
         }
-        if (up.n0 > 0) {
-          lo = min(lo, up.lo0);
-          hi = max(hi, up.lo0 + up.n0);
-        }
-        if (up.n1 > 0) {
-          lo = min(lo, up.lo1);
-          hi = max(hi, up.lo1 + up.n1);
+      } else {
+        for (int k0 = lane; k0 < nz; k0 += 64) {
+          const int k1 = k0 + 32;
+          const float x0 = vox_val(vol, gate_stride, V, cbase + k0);
+          const float x1 = (k1 < nz) ? vox_val(vol, gate_stride, V, cbase + k1) : 0.0f;
+          if (x0 == 0.0f && x1 == 0.0f) continue;
+          UPair up;
+          voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+          if (x0 == 0.0f) up.n0 = 0;
+          if (x1 == 0.0f) up.n1 = 0;
+          const int L = max(up.n0, up.n1);
+          if (L <= 0) continue;
+          const float2 xr = mul2(make_float2(x0, x1), up.rho);
+          float2 Fp = first_edge_prim2(up);
+          float2 lf = f2(1.0f);
+          for (int l = 0; l < L; ++l) {
+            const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+            const float2 w = mul2(add2(F, make_float2(-Fp.x, -Fp.y)), xr);
+            if (l < up.n0) atomicAdd(prof + up.lo0 + l, w.x);
+            if (l < up.n1) atomicAdd(prof + up.lo1 + l, w.y);
+            Fp = F;
+            lf = add2(lf, f2(1.0f));
+          }
+          if (up.n0 > 0) {
+            lo = min(lo, up.lo0);
+            hi = max(hi, up.lo0 + up.n0);
+          }
+          if (up.n1 > 0) {
+            lo = min(lo, up.lo1);
+            hi = max(hi, up.lo1 + up.n1);
+          }
         }
       }
       lo = __reduce_min_sync(FULLM, lo);
       hi = __reduce_max_sync(FULLM, hi);
       __syncwarp();
       if (lo < hi && hi - lo <= 32 * SPREAD_CHUNKS) {
-        // profile read once into registers (and cleared), then one shared
-        // atomic per (row, cell) of the footprint
+        // profile read once into registers (and cleared), then the rows
+        // one at a time
         float pv[SPREAD_CHUNKS];
 #pragma unroll
         for (int q = 0; q < SPREAD_CHUNKS; ++q) {
@@ -110,18 +238,36 @@ __device__ __forceinline__ void band_item(const Params3D &P, const View3D &V,
         }
         for (int r = 0; r < nr; ++r) {
           const float w = wv[r];
-          float *row = acc + (rb - v0 + r) * nu;
+          const int row = rb - v0 + r;
+          float *rowp = acc + row * nu;
+          if (lock_spread) {
+            if (!row_lock(locks + row, err)) continue;
 #pragma unroll
-          for (int q = 0; q < SPREAD_CHUNKS; ++q) {
-            const int u = lo + lane + 32 * q;
-            if (u < hi) atomicAdd(row + u, w * pv[q]);
+            for (int q = 0; q < SPREAD_CHUNKS; ++q) {
+              const int u = lo + lane + 32 * q;
+              if (u < hi) rowp[u] = fmaf(w, pv[q], rowp[u]);
+            }
+            row_unlock(locks + row);
+          } else {
+#pragma unroll
+            for (int q = 0; q < SPREAD_CHUNKS; ++q) {
+              const int u = lo + lane + 32 * q;
+              if (u < hi) atomicAdd(rowp + u, w * pv[q]);
+            }
           }
         }
       } else if (lo < hi) {
         for (int r = 0; r < nr; ++r) {
           const float w = wv[r];
-          float *row = acc + (rb - v0 + r) * nu;
-          for (int u = lo + lane; u < hi; u += 32) atomicAdd(row + u, w * prof[u]);
+          const int row = rb - v0 + r;
+          float *rowp = acc + row * nu;
+          if (lock_spread) {
+            if (!row_lock(locks + row, err)) continue;
+            for (int u = lo + lane; u < hi; u += 32) rowp[u] = fmaf(w, prof[u], rowp[u]);
+            row_unlock(locks + row);
+          } else {
+            for (int u = lo + lane; u < hi; u += 32) atomicAdd(rowp + u, w * prof[u]);
+          }
         }
         __syncwarp();
         for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;

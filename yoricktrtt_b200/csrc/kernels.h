@@ -112,9 +112,14 @@ struct WlsLaunch {
   long long wait_ns;         // bound of that wait
   int *err;
   // filled by launch_wls_persistent
-  int nbands, kchunks, n_band_items, n_col_items;
+  int nbands, kchunks, n_band_items, n_col_items, lock_spread;
 };
 size_t wls_smem(int nu, int band_rows);
+size_t band_fast_smem(int nu, int band_rows, int warps);
+// Spread mode of the band item: row locks for voxel columns of 128 voxels
+// or more, shared atomics below (measured: 256^3 -> 512^2 83 -> 74 ms per
+// 360 views with locks; 128x128x64 -> 256^2 8.4 -> 9.9 ms, so atomics there).
+inline bool band_lock_spread(const Params3D &P) { return P.nz >= 128; }
 int wls_kp(int nz);
 cudaError_t launch_wls_persistent(WlsLaunch L, int sms, cudaStream_t st);
 

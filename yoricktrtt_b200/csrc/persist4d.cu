@@ -71,14 +71,17 @@ k_wls_persistent(const WlsLaunch A)
       float *acc = sm;
       float *prof = sm + R * nu + warp * nu;
       float *wv = sm + R * nu + nwarps * nu + warp * R;
+      int *locks = reinterpret_cast<int *>(sm + R * nu + nwarps * nu + nwarps * R);
       if (threadIdx.x < (int)(sizeof(View3D) / 8))
         reinterpret_cast<double *>(&sV)[threadIdx.x] =
             reinterpret_cast<const double *>(A.views + vi)[threadIdx.x];
       if (threadIdx.x == 0) s_next = 0;
       for (int t = threadIdx.x; t < R * nu; t += blockDim.x) acc[t] = 0.f;
+      for (int t = threadIdx.x; t < R; t += blockDim.x) locks[t] = 0;
       for (int t = lane; t < nu; t += 32) prof[t] = 0.f;
       __syncthreads();
-      band_item<GEOM>(P, sV, A.vol, A.gate_stride, v0, v1, R, acc, prof, wv, &s_next, A.err);
+      band_item<GEOM>(P, sV, A.vol, A.gate_stride, v0, v1, R, acc, prof, wv, locks, &s_next, A.err,
+                      A.lock_spread != 0);
       __syncthreads();
       const long off = (long)vi * nu * nv + (long)v0 * nu;
       const int ncell = (v1 - v0) * nu;
@@ -169,9 +172,10 @@ cudaError_t launch_wls(WlsLaunch L, int sms, cudaStream_t st)
 
 size_t wls_smem(int nu, int band_rows)
 {
-  // band item: band + one profile and one weight row per warp (16 warps);
-  // column items use 16 * nu of it
-  return sizeof(float) * ((size_t)band_rows * nu + 16 * (size_t)nu + 16 * (size_t)band_rows);
+  // band item: band + one profile and one weight row per warp (16 warps) +
+  // one lock per row; column items use 16 * nu of it
+  return sizeof(float) * ((size_t)band_rows * nu + 16 * (size_t)nu + 16 * (size_t)band_rows +
+                          (size_t)band_rows);
 }
 
 int wls_kp(int nz)
@@ -185,6 +189,7 @@ cudaError_t launch_wls_persistent(WlsLaunch L, int sms, cudaStream_t st)
   L.kchunks = (L.P.nz + 64 * kp - 1) / (64 * kp);
   L.nbands = (L.P.nv + L.band_rows - 1) / L.band_rows;
   L.n_band_items = L.nviews * L.nbands;
+  L.lock_spread = band_lock_spread(L.P) ? 1 : 0;
   L.n_col_items = L.ngates * ((L.P.nx * L.P.ny + 15) / 16) * L.kchunks;
   const bool cone = L.P.geom == GEOM_CONE;
   // CTAs per SM: 1 (up to 128 registers per thread) or 2 (64)

@@ -24,7 +24,7 @@ template <int GEOM>
 __global__ void __launch_bounds__(512)
 k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
                   const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
-                  long sino_view_stride, int band_rows, int *__restrict__ err)
+                  long sino_view_stride, int band_rows, int *__restrict__ err, int lock_spread)
 {
   extern __shared__ float sm[];
   __shared__ View3D sV;
@@ -35,6 +35,7 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   float *acc = sm;
   float *prof = sm + band_rows * nu + warp * nu;
   float *wv = sm + band_rows * nu + nwarps * nu + warp * band_rows;
+  int *locks = reinterpret_cast<int *>(sm + band_rows * nu + nwarps * nu + nwarps * band_rows);
   const int vi = blockIdx.y;
   if (threadIdx.x < (int)(sizeof(View3D) / 8))
     reinterpret_cast<double *>(&sV)[threadIdx.x] =
@@ -43,9 +44,11 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   const int v0 = blockIdx.x * band_rows;
   const int v1 = min(v0 + band_rows, nv);
   for (int t = threadIdx.x; t < band_rows * nu; t += blockDim.x) acc[t] = 0.f;
+  for (int t = threadIdx.x; t < band_rows; t += blockDim.x) locks[t] = 0;
   for (int t = lane; t < nu; t += 32) prof[t] = 0.f;
   __syncthreads();
-  band_item<GEOM>(P, sV, vol, gate_stride, v0, v1, band_rows, acc, prof, wv, &s_next, err);
+  band_item<GEOM>(P, sV, vol, gate_stride, v0, v1, band_rows, acc, prof, wv, locks, &s_next, err,
+                  lock_spread != 0);
   __syncthreads();
   float *out = sino + (long)vi * sino_view_stride;
   const int nrow = v1 - v0;
@@ -390,13 +393,13 @@ static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
                                           L.sino_view_stride, L.band_rows, L.err);
     return cudaGetLastError();
   }
-  const size_t smem = sizeof(float) * ((size_t)L.band_rows * L.P.nu + (size_t)L.warps * L.P.nu +
-                                       (size_t)L.warps * L.band_rows);
+  const size_t smem = band_fast_smem(L.P.nu, L.band_rows, L.warps);
   auto kern = k_fwd3d_band_fast<GEOM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<grid, L.warps * 32, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino,
-                                        L.sino_view_stride, L.band_rows, L.err);
+                                        L.sino_view_stride, L.band_rows, L.err,
+                                        band_lock_spread(L.P) ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -428,6 +431,13 @@ cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
 cudaError_t launch_back3d_fast(const Back3DLaunch &L, cudaStream_t st)
 {
   return L.P.geom == GEOM_CONE ? back_fast<GEOM_CONE>(L, st) : back_fast<GEOM_PARALLEL>(L, st);
+}
+
+size_t band_fast_smem(int nu, int band_rows, int warps)
+{
+  // band, one profile and one row-weight list per warp, one lock per row
+  return sizeof(float) * ((size_t)band_rows * nu + (size_t)warps * nu + (size_t)warps * band_rows +
+                          (size_t)band_rows);
 }
 
 }  // namespace trtt

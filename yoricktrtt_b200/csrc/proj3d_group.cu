@@ -32,7 +32,7 @@
 
 #include <climits>
 
-#include "fast3d.cuh"
+#include "fast3d_items.cuh"
 #include "kernels.h"
 
 namespace trtt {
@@ -126,6 +126,29 @@ __device__ __forceinline__ void vec_fma(float2 &b, float w, const float2 &p)
 }
 __device__ __forceinline__ void vec_fma(float &b, float w, const float &p) { b = fmaf(w, p, b); }
 
+// Component M of a cell's member vector, and the vector of G values.
+template <int M> __device__ __forceinline__ float comp(const float4 &v)
+{
+  return M == 0 ? v.x : (M == 1 ? v.y : (M == 2 ? v.z : v.w));
+}
+template <int M> __device__ __forceinline__ float comp(const float2 &v) { return M == 0 ? v.x : v.y; }
+template <int M> __device__ __forceinline__ float comp(const float &v) { return v; }
+__device__ __forceinline__ void pack(float4 &v, const float (&a)[4]) { v = make_float4(a[0], a[1], a[2], a[3]); }
+__device__ __forceinline__ void pack(float2 &v, const float (&a)[2]) { v = make_float2(a[0], a[1]); }
+__device__ __forceinline__ void pack(float &v, const float (&a)[1]) { v = a[0]; }
+
+// S[m] += w * (member m of the cells a0, a1), m < G, packed over the two
+// voxels of a lane.
+template <int G, int M = 0>
+__device__ __forceinline__ void gather_fma(float2 (&S)[G], float2 w, const typename VecOf<G>::T &a0,
+                                           const typename VecOf<G>::T &a1)
+{
+  if constexpr (M < G) {
+    S[M] = fma2(w, make_float2(comp<M>(a0), comp<M>(a1)), S[M]);
+    gather_fma<G, M + 1>(S, w, a0, a1);
+  }
+}
+
 // cell[m] += w * xr[m] for the G interleaved member slots of one profile
 // cell (one vector load, G fused multiply-adds, one vector store).
 template <int G>
@@ -147,70 +170,6 @@ __device__ __forceinline__ void cell_fma(float *cell, float w, const float (&xr)
     *q = v;
   } else {
     *cell = fmaf(w, xr[0], *cell);
-  }
-}
-
-// True when floor(uc_k - hs_k), the first cell of voxel k's u-footprint
-// before any clamp, strictly increases or decreases along the column: the
-// voxels of one warp step then write distinct cells at every footprint
-// offset l, so a warp can update its profile with plain loads and stores.
-// |d uc/dk| = |B|; hs = hs0 h_u0 magn delta_u varies by at most
-// hs0 h_u0m |B| max|uc - a12| u_scl^2 inv_den per voxel.
-template <int GEOM>
-__device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D &V,
-                                                const ColGeo<MODEL_CUBIC> &c)
-{
-  const double b = fabs(c.B);
-  if constexpr (GEOM == GEOM_CONE) {
-    const double ua = c.A, ub = fma(c.B, (double)(P.nz - 1), c.A);
-    const double um = fmax(fabs(ua - V.a12), fabs(ub - V.a12));
-    const double dhs = P.hs0 * (double)c.h_u0m * b * um * P.u_scl * P.u_scl * (double)c.inv_den;
-    return b - dhs >= 1.002;
-  } else {
-    return b >= 1.002;
-  }
-}
-
-__device__ __forceinline__ unsigned long long timer_ns()
-{
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Exclusive use of one band row by a warp (lane 0 takes the lock, the warp
-// then updates the row with plain loads and stores).  The wait is bounded:
-// past 2 s the warp sets TRTT_ERR_STALL and skips the row.  A holder
-// releases after a few hundred cycles, so the limit is never reached in a
-// correct run.
-__device__ __forceinline__ bool row_lock(int *lock, int *err)
-{
-  int got = 1;
-  if ((threadIdx.x & 31) == 0) {
-    if (atomicCAS(lock, 0, 1) != 0) {
-      const unsigned long long t0 = timer_ns();
-      while (atomicCAS(lock, 0, 1) != 0) {
-        if (timer_ns() - t0 > 2000000000ull) {
-          atomicOr(err, TRTT_ERR_STALL);
-          got = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence_block();
-  }
-  got = __shfl_sync(FULLM, got, 0);
-  __syncwarp();
-  return got != 0;
-}
-
-__device__ __forceinline__ void row_unlock(int *lock)
-{
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) {
-    __threadfence_block();
-    atomicExch(lock, 0);
   }
 }
 
@@ -316,6 +275,7 @@ k_fwd3d_group(const GroupFwdLaunch A)
             x[m].y = (k1 < khi) ? __ldg(colp[m] + k1) : 0.0f;
             any = any || x[m].x != 0.0f || x[m].y != 0.0f;
           }
+          if (!__any_sync(FULLM, any)) continue;
           UPair up;
           voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
           if (k0 >= khi || !any) up.n0 = 0;
@@ -539,14 +499,17 @@ template <int GEOM, int G, int KP>
 __global__ void __launch_bounds__(256, 2)
 k_back3d_group(const GroupBackLaunch A)
 {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   const Params3D &P = A.P;
   const int nwarps = blockDim.x >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nu = P.nu, nz = P.nz, nx = P.nx, ny = P.ny;
   const int orbit = blockIdx.x * nwarps + warp;
   if (orbit >= A.norbits) return;
-  float *Q = sm + warp * G * nu;  // [G][nu], this warp
+  using VecG = typename VecOf<G>::T;
+  // v-collapsed member profiles, interleaved: cell u's G member values at
+  // Q[u] (this warp's nu cells)
+  VecG *Q = reinterpret_cast<VecG *>(sm) + warp * nu;
   int i0, j0;
   orbit_rep<G>(orbit, nx, ny, i0, j0);
   int oi[G], oj[G];
@@ -652,12 +615,21 @@ k_back3d_group(const GroupBackLaunch A)
               }
             }
 #pragma unroll
-            for (int m = 0; m < G; ++m)
+            for (int c = 0; c < QV; ++c) {
+              const int u = ub + 4 * lane + 128 * c;
+              if (u < a1) {
+                float v[4][G];
 #pragma unroll
-              for (int c = 0; c < QV; ++c) {
-                const int u = ub + 4 * lane + 128 * c;
-                if (u < a1) *reinterpret_cast<float4 *>(Q + m * nu + u) = q[m][c];
+                for (int m = 0; m < G; ++m) {
+                  v[0][m] = comp<0>(q[m][c]);
+                  v[1][m] = comp<1>(q[m][c]);
+                  v[2][m] = comp<2>(q[m][c]);
+                  v[3][m] = comp<3>(q[m][c]);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) pack(Q[u + j], v[j]);
               }
+            }
           }
         } else {
         constexpr int QC = G == 4 ? 4 : 8;
@@ -685,10 +657,13 @@ k_back3d_group(const GroupBackLaunch A)
             }
           }
 #pragma unroll
-          for (int m = 0; m < G; ++m)
+          for (int c = 0; c < QC; ++c)
+            if (ub + lane + 32 * c < hi) {
+              float v[G];
 #pragma unroll
-            for (int c = 0; c < QC; ++c)
-              if (ub + lane + 32 * c < hi) Q[m * nu + ub + lane + 32 * c] = q[m][c];
+              for (int m = 0; m < G; ++m) v[m] = q[m][c];
+              pack(Q[ub + lane + 32 * c], v);
+            }
         }
         }
         __syncwarp();
@@ -703,17 +678,14 @@ k_back3d_group(const GroupBackLaunch A)
 #pragma unroll
           for (int m = 0; m < G; ++m) S[m] = f2(0.f);
           float2 lf = f2(1.0f);
-          const float *q0 = Q + up[kp].lo0;
-          const float *q1 = Q + up[kp].lo1;
+          const VecG *q0 = Q + up[kp].lo0;
+          const VecG *q1 = Q + up[kp].lo1;
           for (int l = 0; l < L; ++l) {
             const float2 F = cubic_prim2(fma2(lf, up[kp].inc, up[kp].start));
             const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
-#pragma unroll
-            for (int m = 0; m < G; ++m) {
-              const float a0 = (l < up[kp].n0) ? q0[m * nu + l] : 0.0f;
-              const float a1 = (l < up[kp].n1) ? q1[m * nu + l] : 0.0f;
-              S[m] = fma2(w, make_float2(a0, a1), S[m]);
-            }
+            const VecG a0 = (l < up[kp].n0) ? q0[l] : VecG{};
+            const VecG a1 = (l < up[kp].n1) ? q1[l] : VecG{};
+            gather_fma<G>(S, w, a0, a1);
             Fp = F;
             lf = add2(lf, f2(1.0f));
           }
