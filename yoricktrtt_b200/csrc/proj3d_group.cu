@@ -106,6 +106,30 @@ __device__ __forceinline__ void column_k_range(const ColGeo<MODEL_CUBIC> &c, dou
   khi = (int)kb;
 }
 
+// cell[m] += w.x * xa[m] + w.y * xc[m] for the G interleaved member slots
+// of one profile cell (the two voxels of a lane).
+template <int G>
+__device__ __forceinline__ void cell_fma2(float *cell, float2 w, const float (&xa)[G], const float (&xc)[G])
+{
+  if constexpr (G == 4) {
+    float4 *q = reinterpret_cast<float4 *>(cell);
+    float4 v = *q;
+    v.x = fmaf(w.y, xc[0], fmaf(w.x, xa[0], v.x));
+    v.y = fmaf(w.y, xc[1], fmaf(w.x, xa[1], v.y));
+    v.z = fmaf(w.y, xc[2], fmaf(w.x, xa[2], v.z));
+    v.w = fmaf(w.y, xc[3], fmaf(w.x, xa[3], v.w));
+    *q = v;
+  } else if constexpr (G == 2) {
+    float2 *q = reinterpret_cast<float2 *>(cell);
+    float2 v = *q;
+    v.x = fmaf(w.y, xc[0], fmaf(w.x, xa[0], v.x));
+    v.y = fmaf(w.y, xc[1], fmaf(w.x, xa[1], v.y));
+    *q = v;
+  } else {
+    *cell = fmaf(w.y, xc[0], fmaf(w.x, xa[0], *cell));
+  }
+}
+
 // The G member values of one interleaved profile or band cell.
 template <int G> struct VecOf;
 template <> struct VecOf<4> { using T = float4; };
@@ -146,30 +170,6 @@ __device__ __forceinline__ void gather_fma(float2 (&S)[G], float2 w, const typen
   if constexpr (M < G) {
     S[M] = fma2(w, make_float2(comp<M>(a0), comp<M>(a1)), S[M]);
     gather_fma<G, M + 1>(S, w, a0, a1);
-  }
-}
-
-// cell[m] += w * xr[m] for the G interleaved member slots of one profile
-// cell (one vector load, G fused multiply-adds, one vector store).
-template <int G>
-__device__ __forceinline__ void cell_fma(float *cell, float w, const float (&xr)[G])
-{
-  if constexpr (G == 4) {
-    float4 *q = reinterpret_cast<float4 *>(cell);
-    float4 v = *q;
-    v.x = fmaf(w, xr[0], v.x);
-    v.y = fmaf(w, xr[1], v.y);
-    v.z = fmaf(w, xr[2], v.z);
-    v.w = fmaf(w, xr[3], v.w);
-    *q = v;
-  } else if constexpr (G == 2) {
-    float2 *q = reinterpret_cast<float2 *>(cell);
-    float2 v = *q;
-    v.x = fmaf(w, xr[0], v.x);
-    v.y = fmaf(w, xr[1], v.y);
-    *q = v;
-  } else {
-    *cell = fmaf(w, xr[0], *cell);
   }
 }
 
@@ -261,40 +261,47 @@ k_fwd3d_group(const GroupFwdLaunch A)
       // side by side; member m of cell c at prof[c * G + m], else prof[m U + c]
       const int cs = IL ? G : 1, ms = IL ? 1 : U;
       if (IL && column_monotone<GEOM>(P, V, cc)) {
-        // plain loads and stores: every voxel walks its footprint from the
-        // unclamped first cell (where the primitive is 0), writing cells
-        // inside [u0, e); at each step the warp's 64 voxels write 64
-        // distinct cells, and the steps are ordered by __syncwarp
+        // plain loads and stores.  Lane j takes the adjacent voxels 2j and
+        // 2j+1 of the step (a: the one whose footprint starts lower, c: the
+        // other) and walks cells f_a, f_a + 1, ... from a's unclamped first
+        // cell (where the primitive is 0), adding a's weight at offset l and
+        // c's at l - d (d = f_c - f_a >= 1) in one update of the cell.  The
+        // first cells of the 32 lanes' pairs are at least 2 apart, so at
+        // each step the warp writes 32 distinct cells; steps are ordered by
+        // __syncwarp.  Cells left of the tile are not written (c >= u0).
+        const int sa = cc.B > 0.0 ? 0 : 1;
         for (int kb = klo; kb < khi; kb += 64) {
-          const int k0 = kb + lane, k1 = k0 + 32;
+          const int ka = kb + 2 * lane + sa, kc = kb + 2 * lane + (1 - sa);
           float2 x[G];
           bool any = false;
 #pragma unroll
           for (int m = 0; m < G; ++m) {
-            x[m].x = (k0 < khi) ? __ldg(colp[m] + k0) : 0.0f;
-            x[m].y = (k1 < khi) ? __ldg(colp[m] + k1) : 0.0f;
+            x[m].x = (ka < khi) ? __ldg(colp[m] + ka) : 0.0f;
+            x[m].y = (kc < khi) ? __ldg(colp[m] + kc) : 0.0f;
             any = any || x[m].x != 0.0f || x[m].y != 0.0f;
           }
           if (!__any_sync(FULLM, any)) continue;
           UPair up;
-          voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
-          if (k0 >= khi || !any) up.n0 = 0;
-          if (k1 >= khi || !any) up.n1 = 0;
-          const double uc0 = fma(cc.B, (double)k0, cc.A), uc1 = fma(cc.B, (double)k1, cc.A);
+          voxel_u_pair<GEOM>(P, V, cc, ka, kc, up);
+          if (ka >= khi || !any) up.n0 = 0;
+          if (kc >= khi || !any) up.n1 = 0;
+          const double uc0 = fma(cc.B, (double)ka, cc.A), uc1 = fma(cc.B, (double)kc, cc.A);
           const float2 hsv = mul2(make_float2(__frcp_rn(up.inc.x), __frcp_rn(up.inc.y)),
                                   f2((float)P.hs0));
           const int f0 = __double2int_rd(uc0 - (double)hsv.x), f1 = __double2int_rd(uc1 - (double)hsv.y);
           // the reference's first cell is f clamped to [0, nu-1]: cells left
-          // of the tile are not written (c >= u0 below); a footprint that
-          // starts past the detector (f >= nu) gives its one clamped cell
-          // weight 0 - 0 and is dropped.  Where hs rounds f one cell away
-          // from the reference's lo, the cell between holds a weight below
-          // the primitive's value within 1e-6 of the support end (~1e-27).
+          // of the tile are not written; a footprint that starts past the
+          // detector (f >= nu) gives its one clamped cell weight 0 - 0 and is
+          // dropped.  Where hs rounds f one cell away from the reference's
+          // lo, the cell between holds a weight below the primitive's value
+          // within 1e-6 of the support end (~1e-27).
           const int e0 = up.n0 > 0 ? min(up.lo0 + up.n0, u1) : INT_MIN;
           const int e1 = up.n1 > 0 ? min(up.lo1 + up.n1, u1) : INT_MIN;
           const int L0 = (up.n0 > 0 && f0 < nu) ? max(e0 - f0, 0) : 0;
           const int L1 = (up.n1 > 0 && f1 < nu) ? max(e1 - f1, 0) : 0;
-          const int Lw = __reduce_max_sync(FULLM, max(max(L0, L1), 0));
+          const int d = f1 - f0;
+          const int Ln = max(L0, L1 > 0 ? d + L1 : 0);
+          const int Lw = __reduce_max_sync(FULLM, Ln);
           if (Lw <= 0) continue;
           const float2 start = make_float2(fmaf((float)(f0 - up.lo0), up.inc.x, up.start.x),
                                            fmaf((float)(f1 - up.lo1), up.inc.y, up.start.y));
@@ -306,13 +313,15 @@ k_fwd3d_group(const GroupFwdLaunch A)
             xr1[m] = t.y;
           }
           float2 Fp = f2(0.0f);
-          float2 lf = f2(1.0f);
+          float2 lf = make_float2(1.0f, (float)(1 - d));
           for (int l = 0; l < Lw; ++l) {
             const float2 F = cubic_prim2(fma2(lf, up.inc, start));
-            const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
-            const int c0 = f0 + l, c1 = f1 + l;
-            if (l < L0 && c0 >= u0) cell_fma<G>(prof + (c0 - u0) * G, w.x, xr0);
-            if (l < L1 && c1 >= u0) cell_fma<G>(prof + (c1 - u0) * G, w.y, xr1);
+            float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+            const bool on0 = l < L0, on1 = l >= d && l - d < L1;
+            if (!on0) w.x = 0.0f;
+            if (!on1) w.y = 0.0f;
+            const int c = f0 + l;
+            if ((on0 || on1) && c >= u0) cell_fma2<G>(prof + (c - u0) * G, w, xr0, xr1);
             __syncwarp();
             Fp = F;
             lf = add2(lf, f2(1.0f));
