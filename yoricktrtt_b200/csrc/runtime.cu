@@ -72,7 +72,16 @@ cudaError_t DropIn::init()
   if (e != cudaSuccess) return e;
   e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;
-  e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking);
+  // The copy stream also runs the small FP32 <-> FP64 conversion kernels
+  // between its copies.  The projector kernels occupy every SM (one CTA of
+  // up to 219 KB of shared memory per SM), so at default priority a
+  // conversion waited for a whole kernel to drain and the copies fell behind
+  // (11 ms of trailing copies after a 360-view direct projection); at the
+  // greatest priority it takes the next SM that frees up.
+  int prio_least = 0, prio_greatest = 0;
+  e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamCreateWithPriority(&copy, cudaStreamNonBlocking, prio_greatest);
   if (e != cudaSuccess) return e;
   e = cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking);
   if (e != cudaSuccess) return e;

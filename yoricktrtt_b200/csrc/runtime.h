@@ -37,7 +37,7 @@ struct DropIn {
   bool ready = false;
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t copy = nullptr;  // host<->device copies that overlap the kernels
+  cudaStream_t copy = nullptr;  // host<->device copies that overlap the kernels (greatest priority)
   cudaStream_t stream2 = nullptr;  // second kernel stream: view chunks of the direct projection
   int sms = 148;                 // streaming multiprocessors of `device`
   // ev[0], ev[1]: copy stream start / end; ev[2 + c]: view chunk c (at most
