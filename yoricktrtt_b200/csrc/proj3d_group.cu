@@ -222,15 +222,18 @@ k_fwd3d_group(const GroupFwdLaunch A)
     const int mycol = (chunk << 5) + lane;
     ColGeo<MODEL_CUBIC> c;
     bool hit = false;
+    // per column, by its own lane: the voxel range whose footprints may meet
+    // the u tile and the monotone test (shuffled to the warp for each hit)
+    int my_klo = 0, my_khi = nz, my_mono = 0;
     if (mycol < ncols) {
       column_geo<GEOM, MODEL_CUBIC>(P, V, mycol % nx, mycol / nx, 0, c);
       if (c.bad) atomicOr(A.err, TRTT_ERR_SOURCE_PLANE);
       hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
       if (hit && A.usplit > 1) {
-        int klo, khi;
-        column_k_range(c, column_u_halfwidth<GEOM>(P, V, c), u0, u1, nz, klo, khi);
-        hit = klo < khi;
+        column_k_range(c, column_u_halfwidth<GEOM>(P, V, c), u0, u1, nz, my_klo, my_khi);
+        hit = my_klo < my_khi;
       }
+      if (IL && hit) my_mono = column_monotone<GEOM>(P, V, c) ? 1 : 0;
     }
     unsigned mask = __ballot_sync(FULLM, hit);
     while (mask) {
@@ -251,16 +254,13 @@ k_fwd3d_group(const GroupFwdLaunch A)
       const int vl = cc.vax.lo, vr = cc.vax.lo + cc.vax.n;
       const int rb = max(vl, v0), re = min(vr, v1), nr = re - rb;
       for (int r = lane; r < nr; r += 32) wv[r] = axis_weight<MODEL_CUBIC>(cc.vax, rb - vl + r, P);
-      int klo = 0, khi = nz;
-      if (A.usplit > 1) {
-        const double hsm = column_u_halfwidth<GEOM>(P, V, cc);
-        column_k_range(cc, hsm, u0, u1, nz, klo, khi);
-      }
+      const int klo = __shfl_sync(FULLM, my_klo, src), khi = __shfl_sync(FULLM, my_khi, src);
+      const bool mono = __shfl_sync(FULLM, my_mono, src) != 0;
       int lo = INT_MAX, hi = INT_MIN;
       // interleaved profiles (IL): cell-major, the G member values of a cell
       // side by side; member m of cell c at prof[c * G + m], else prof[m U + c]
       const int cs = IL ? G : 1, ms = IL ? 1 : U;
-      if (IL && column_monotone<GEOM>(P, V, cc)) {
+      if (IL && mono) {
         // plain loads and stores.  Lane j takes the adjacent voxels 2j and
         // 2j+1 of the step (a: the one whose footprint starts lower, c: the
         // other) and walks cells f_a, f_a + 1, ... from a's unclamped first
