@@ -272,11 +272,11 @@ int trtt_b200_plan3d_factorized(const trtt_b200_plan3d *plan);
  * quads found (all-zero when the group kernels never apply to the plan).
  * set_symmetry(plan, 0) returns to the per-view kernels (results equal to
  * FP32 summation order); 2 (default) uses the group kernels with the member
- * profiles of the direct projector interleaved per detector cell and
- * updated by plain shared-memory loads and stores wherever the voxels'
- * first cells strictly increase along a column (1.5x faster than 1 at
- * 256^3 -> 360 x 512^2); 1 the group kernels with one profile per member
- * and shared-memory atomics. */
+ * profiles and bands of the direct projector interleaved per detector cell,
+ * profiles updated by plain shared-memory loads and stores wherever the
+ * voxels' first cells strictly increase along a column and band rows under
+ * row locks (35.7 ms per 360 views at 256^3 -> 512^2); 1 the group kernels
+ * with one profile per member and shared-memory atomics (87 ms). */
 int trtt_b200_plan3d_groups(const trtt_b200_plan3d *plan, long *counts);
 int trtt_b200_plan3d_set_symmetry(trtt_b200_plan3d *plan, int on);
 
@@ -289,8 +289,9 @@ int trtt_b200_plan3d_set_group_tiles(trtt_b200_plan3d *plan, int band_rows4, int
                                      int band_rows1, long back_chunk_bytes);
 /* Shape of the direct kernel for groups of 4 views: band rows (0 keeps),
  * detector cells per u tile (0: up to 256; else 32..256) and CTAs per SM
- * (1: up to 128 registers per thread, 2: 64; 0 keeps).  -1 if the CTA's
- * shared memory does not fit at that occupancy. */
+ * (1: one CTA of 22 warps, or 16 where 22 warps' profiles do not fit in
+ * shared memory; 2: two CTAs of 16 warps, 64 registers per thread; 0
+ * keeps).  -1 if the CTA's shared memory does not fit at that occupancy. */
 int trtt_b200_plan3d_set_group_shape(trtt_b200_plan3d *plan, int band_rows4, int utile4,
                                      int ctas_per_sm4);
 
