@@ -623,7 +623,7 @@ void member_runs(const std::vector<int> &list, int G, long g0, long g1,
 // stream, ordered after ev[0].
 int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
                    const std::vector<int> (&lists)[3], long nviews, int job,
-                   const std::function<cudaError_t(cudaStream_t)> &out_to_device)
+                   const std::function<cudaError_t(cudaStream_t)> &out_to_device, bool in_early)
 {
   cudaStream_t st = D.stream, cp = D.copy, ks2 = D.stream2;
   const long nx = P.nx, ny = P.ny, nz = P.nz, nu = P.nu, nv = P.nv;
@@ -643,7 +643,10 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
   std::vector<std::pair<long, long>> runs;
   int ev = 2;
   if (job == 0) {
-    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nvox, cudaMemcpyHostToDevice, st));
+    if (in_early)  // started on the copy stream before the grouping
+      TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvIn], 0));
+    else
+      TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nvox, cudaMemcpyHostToDevice, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
@@ -669,7 +672,12 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
       L.err = D.err.as<int>();
       const long bands = (nv + L.band_rows - 1) / L.band_rows;
       const long per_wave = (long)D.sms * (G == 4 ? 1 : 2);
-      const std::vector<long> cb = fwd_chunks(n, (n + 5) / 6, std::max<long>(1, per_wave / (bands * usplit)), 10);
+      // chunks of at most ~84 MB of FP64 output (1.5 ms of read-back at
+      // ~57 GB/s), so that the read-back of the last full chunk hides behind
+      // the last, one-wave chunk (measured at 256^3 -> 360 x 512^2: chunks of
+      // 10 quads 39.4 ms per call, of 15 quads 40.1-42.3 ms)
+      const long per_chunk = std::max<long>(1, std::min<long>((n + 5) / 6, 84000000L / (G * nview_px * 8)));
+      const std::vector<long> cb = fwd_chunks(n, per_chunk, std::max<long>(1, per_wave / (bands * usplit)), 12);
       for (size_t c = 0; c + 1 < cb.size(); ++c, ++unit) {
         cudaStream_t ks = (unit & 1) ? ks2 : st;
         L.groups = D.grp.as<int>() + offs[q] + 4 * cb[c];
@@ -790,6 +798,13 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     if (accumulate) return cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);
     return cudaMemsetAsync(D.out64.p, 0, sizeof(double) * nout, s);
   };
+  // the factorised closed-form direct projection starts from the volume:
+  // its upload overlaps the view grouping and the source-plane check below
+  const bool in_early = job == 0 && fact && !cum;
+  if (in_early) {
+    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvIn], cp));
+  }
   std::vector<int> glists[3];
   bool grouped = false;
   if (fact && !cum && nviews <= 65535) {
@@ -805,13 +820,14 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     TRTT_CK(cudaStreamSynchronize(st));
     if (herr & TRTT_ERR_SOURCE_PLANE) {
+      TRTT_CK(cudaStreamSynchronize(cp));  // the early upload still reads `in`
       std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
       return fail("a voxel lies in the source plane (wk == 0)");
     }
-    return host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device);
+    return host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device, in_early);
   }
   if (grouped) {
-    const int r = host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device);
+    const int r = host3d_grouped(D, P, out, in, glists, nviews, job, out_to_device, in_early);
     if (r < 0) return r;
   } else if (job == 0 && fact) {
     // Column-factorised views: the only failure (a voxel in the source
@@ -825,10 +841,14 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     TRTT_CK(cudaMemcpyAsync(&herr, D.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     TRTT_CK(cudaStreamSynchronize(st));
     if (herr & TRTT_ERR_SOURCE_PLANE) {
+      TRTT_CK(cudaStreamSynchronize(cp));  // the early upload still reads `in`
       std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
       return fail("a voxel lies in the source plane (wk == 0)");
     }
-    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+    if (in_early)
+      TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvIn], 0));
+    else
+      TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));

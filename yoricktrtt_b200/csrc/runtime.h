@@ -41,9 +41,11 @@ struct DropIn {
   cudaStream_t stream2 = nullptr;  // second kernel stream: view chunks of the direct projection
   int sms = 148;                 // streaming multiprocessors of `device`
   // ev[0], ev[1]: copy stream start / end; ev[2 + c]: view chunk c (at most
-  // kChunks); ev[kEvents - 2], ev[kEvents - 1]: second kernel stream start / end
+  // kChunks); ev[kEvIn]: the input upload started early on the copy stream;
+  // ev[kEvents - 2], ev[kEvents - 1]: second kernel stream start / end
   static constexpr int kChunks = 31;
-  static constexpr int kEvents = kChunks + 4;
+  static constexpr int kEvIn = kChunks + 2;
+  static constexpr int kEvents = kChunks + 5;
   cudaEvent_t ev[kEvents] = {};
   DevBuf in64, out64, vol32, det32, geom, gates, aux, err, grp;
   cudaError_t init();
