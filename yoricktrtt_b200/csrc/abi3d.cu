@@ -34,7 +34,7 @@ struct trtt_b200_plan3d {
   int tc = 0;    // 1: tensor-core band kernel (closed-form model)
   int cols = 1;  // 2: column-pair band kernel (closed-form model)
   bool factorized = true;
-  DevBuf views, cum, gate_ptr, entries, scratch, err;
+  DevBuf views, cum, gate_ptr, entries, pairs, scratch, err;
   std::vector<View3D> hviews;
   // view groups related by turns of the grid (closed-form model, factorised
   // views): index 0 singles, 1 pairs (half turns), 2 quads (quarter turns)
@@ -76,6 +76,21 @@ static int upload_gates(trtt_b200_plan3d *pl, const std::vector<std::vector<Gate
   TRTT_CK(cudaMemcpy(pl->gate_ptr.p, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
   if (!ent.empty())
     TRTT_CK(cudaMemcpy(pl->entries.p, ent.data(), sizeof(GateEntry) * ent.size(), cudaMemcpyHostToDevice));
+  // the same weights by view, for the transpose that walks each view once
+  std::vector<GatePair> pairs(std::max<long>(1, pl->nviews), GatePair{-1, -1, 0.f, 0.f});
+  for (size_t g = 0; g < lists.size(); ++g)
+    for (const GateEntry &e : lists[g]) {
+      GatePair &q = pairs[e.view];
+      if (q.g0 < 0) {
+        q.g0 = (int)g;
+        q.w0 = e.w;
+      } else {
+        q.g1 = (int)g;
+        q.w1 = e.w;
+      }
+    }
+  TRTT_CK(pl->pairs.ensure(sizeof(GatePair) * pairs.size()));
+  TRTT_CK(cudaMemcpy(pl->pairs.p, pairs.data(), sizeof(GatePair) * pairs.size(), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -502,6 +517,7 @@ static int plan_run(trtt_b200_plan3d *pl, const float *src, float *dst, long vie
     L.vol = volo;
     L.gate_stride = nvox;
     L.factorized = pl->factorized ? 1 : 0;
+    L.pairs = pl->nt > 1 ? pl->pairs.as<GatePair>() : nullptr;
     L.err = pl->err.as<int>();
     TRTT_CK(launch_back3d(L, st));
     count_launch();
@@ -546,6 +562,7 @@ extern "C" int trtt_b200_plan3d_destroy(trtt_b200_plan3d *pl)
   pl->cum.release();
   pl->gate_ptr.release();
   pl->entries.release();
+  pl->pairs.release();
   for (auto &gb : pl->groups) gb.release();
   pl->resid.release();
   pl->wls_parts.release();

@@ -289,6 +289,137 @@ struct LoadCG {
   __device__ __forceinline__ static float4 ld4(const float4 *p) { return __ldcg(p); }
 };
 
+// One view's contribution to the voxels kbase + lane + 64 p (+32), p < KP,
+// of column (i, j): term[p] = rho * sum_u w(u) Q[u] for the lane's two
+// voxels, with Q[u] = sum_v wv(v) img[v][u] the column's v-collapsed profile
+// of the view's image `img0`, built in this warp's nu-float row Q.  cc is
+// the column's geometry in the view.  Returns false (term untouched, Q not
+// used) when the footprints of the warp's voxels miss the detector.  vec4:
+// nu % 4 == 0 and 16-byte aligned images (16-byte loads).  All lanes call it.
+template <int GEOM, int KP, class LD>
+__device__ __forceinline__ bool view_gather(const Params3D &P, const View3D &V,
+                                            const ColGeo<MODEL_CUBIC> &cc, int kbase,
+                                            const float *img0, float *Q, bool vec4,
+                                            float2 (&term)[KP])
+{
+  const int lane = threadIdx.x & 31;
+  const int nu = P.nu, nz = P.nz;
+  UPair up[KP];
+  int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
+    voxel_u_pair<GEOM>(P, V, cc, k0, k1, up[p]);
+    if (k0 >= nz) up[p].n0 = 0;
+    if (k1 >= nz) up[p].n1 = 0;
+    if (up[p].n0 > 0) {
+      lo = min(lo, up[p].lo0);
+      hi = max(hi, up[p].lo0 + up[p].n0);
+    }
+    if (up[p].n1 > 0) {
+      lo = min(lo, up[p].lo1);
+      hi = max(hi, up[p].lo1 + up[p].n1);
+    }
+  }
+  lo = __reduce_min_sync(FULLM, lo);
+  hi = __reduce_max_sync(FULLM, hi);
+  if (lo >= hi) return false;
+  // v-collapsed profile Q[u] = sum_v wv(v) pix[v][u], u in [lo, hi).
+  // Each lane keeps up to QC cells of Q in registers (u = lo + lane + 32c)
+  // and walks the footprint rows; the QC loads of a row are independent,
+  // so a warp keeps many loads in flight.
+  const int npv = cc.vax.n;
+  if (vec4) {
+    // cover [lo & ~3, hi rounded up to 4): 16-byte loads, packed FMAs
+    constexpr int QV = 4;
+    const int a0 = lo & ~3, a1 = (hi + 3) & ~3;
+    for (int ub = a0; ub < a1; ub += 128 * QV) {
+      float4 q[QV];
+#pragma unroll
+      for (int c = 0; c < QV; ++c) q[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int m0 = 0; m0 < npv; m0 += 32) {
+        const int mn = min(32, npv - m0);
+        const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+        for (int m = 0; m < mn; ++m) {
+          const float2 w = f2(__shfl_sync(FULLM, wl, m));
+          const float4 *row =
+              reinterpret_cast<const float4 *>(img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + 4 * lane);
+          float4 a[QV];
+#pragma unroll
+          for (int c = 0; c < QV; ++c)
+            a[c] = (ub + 4 * lane + 128 * c < a1) ? LD::ld4(row + 32 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+          for (int c = 0; c < QV; ++c) {
+            const float2 l2 = fma2(w, make_float2(a[c].x, a[c].y), make_float2(q[c].x, q[c].y));
+            const float2 h2 = fma2(w, make_float2(a[c].z, a[c].w), make_float2(q[c].z, q[c].w));
+            q[c] = make_float4(l2.x, l2.y, h2.x, h2.y);
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < QV; ++c) {
+        const int u = ub + 4 * lane + 128 * c;
+        if (u < a1) *reinterpret_cast<float4 *>(Q + u) = q[c];
+      }
+    }
+  } else {
+    constexpr int QC = 16;
+    for (int ub = lo; ub < hi; ub += 32 * QC) {
+      float q[QC];
+#pragma unroll
+      for (int c = 0; c < QC; ++c) q[c] = 0.f;
+      for (int m0 = 0; m0 < npv; m0 += 32) {
+        const int mn = min(32, npv - m0);
+        const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+        for (int m = 0; m < mn; ++m) {
+          const float w = __shfl_sync(FULLM, wl, m);
+          const float *row = img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + lane;
+          float a[QC];
+#pragma unroll
+          for (int c = 0; c < QC; ++c) a[c] = (ub + lane + 32 * c < hi) ? LD::ld(row + 32 * c) : 0.f;
+#pragma unroll
+          for (int c = 0; c < QC; ++c) q[c] = fmaf(w, a[c], q[c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < QC; ++c)
+        if (ub + lane + 32 * c < hi) Q[ub + lane + 32 * c] = q[c];
+    }
+  }
+  __syncwarp();
+  // per-voxel gathers, two voxels per instruction
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    term[p] = f2(0.f);
+    const int L = max(up[p].n0, up[p].n1);
+    if (L <= 0) continue;
+    float2 Fp = first_edge_prim2(up[p]);
+    float2 S = f2(0.f);
+    float2 lf = f2(1.0f);
+    for (int l = 0; l < L; ++l) {
+      const float2 F = cubic_prim2(fma2(lf, up[p].inc, up[p].start));
+      const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+      const float q0 = (l < up[p].n0) ? Q[up[p].lo0 + l] : 0.0f;
+      const float q1 = (l < up[p].n1) ? Q[up[p].lo1 + l] : 0.0f;
+      S = fma2(w, make_float2(q0, q1), S);
+      Fp = F;
+      lf = add2(lf, f2(1.0f));
+    }
+    term[p] = mul2(up[p].rho, S);
+  }
+  __syncwarp();  // Q is free for the next view
+  return true;
+}
+
+// Packed Kahan step: acc += term with compensation cmp.
+__device__ __forceinline__ void kahan2(float2 &acc, float2 &cmp, float2 term)
+{
+  const float2 y = add2(term, make_float2(-cmp.x, -cmp.y));
+  const float2 t = add2(acc, y);
+  cmp = add2(add2(t, make_float2(-acc.x, -acc.y)), make_float2(-y.x, -y.y));
+  acc = t;
+}
+
 // Column item.  One warp: column col = (i, j), voxels kbase + lane + 64 p
 // (+32), p < KP, gate `gate`; the entries [e0, e1) of the gate's list with
 // views in [view_lo, view_hi) (images at sino[view - view_lo]).  Q: this
@@ -304,7 +435,7 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
                                             int *__restrict__ err, bool vec4 = false)
 {
   const int lane = threadIdx.x & 31;
-  const int nu = P.nu, nz = P.nz;
+  const int nz = P.nz;
   const int i = col % P.nx, j = col / P.nx;
   float2 acc[KP], cmp[KP];
 #pragma unroll
@@ -335,116 +466,12 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
       const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
       const int view = __shfl_sync(FULLM, myview, s);
       const float wgt = __shfl_sync(FULLM, myw, s);
-      const View3D &V = views[view];
-      UPair up[KP];
-      int lo = INT_MAX, hi = INT_MIN;
+      float2 term[KP];
+      if (!view_gather<GEOM, KP, LD>(P, views[view], cc, kbase,
+                                     sino + (long)(view - view_lo) * sino_view_stride, Q, vec4, term))
+        continue;
 #pragma unroll
-      for (int p = 0; p < KP; ++p) {
-        const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
-        voxel_u_pair<GEOM>(P, V, cc, k0, k1, up[p]);
-        if (k0 >= nz) up[p].n0 = 0;
-        if (k1 >= nz) up[p].n1 = 0;
-        if (up[p].n0 > 0) {
-          lo = min(lo, up[p].lo0);
-          hi = max(hi, up[p].lo0 + up[p].n0);
-        }
-        if (up[p].n1 > 0) {
-          lo = min(lo, up[p].lo1);
-          hi = max(hi, up[p].lo1 + up[p].n1);
-        }
-      }
-      lo = __reduce_min_sync(FULLM, lo);
-      hi = __reduce_max_sync(FULLM, hi);
-      if (lo >= hi) continue;
-      // v-collapsed profile Q[u] = sum_v wv(v) pix[v][u], u in [lo, hi).
-      // Each lane keeps up to QC cells of Q in registers (u = lo + lane + 32c)
-      // and walks the footprint rows; the QC loads of a row are independent,
-      // so a warp keeps many loads in flight.
-      const int npv = cc.vax.n;
-      const float *img0 = sino + (long)(view - view_lo) * sino_view_stride;
-      if (vec4) {
-        // cover [lo & ~3, hi rounded up to 4): 16-byte loads, packed FMAs
-        constexpr int QV = 4;
-        const int a0 = lo & ~3, a1 = (hi + 3) & ~3;
-        for (int ub = a0; ub < a1; ub += 128 * QV) {
-          float4 q[QV];
-#pragma unroll
-          for (int c = 0; c < QV; ++c) q[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-          for (int m0 = 0; m0 < npv; m0 += 32) {
-            const int mn = min(32, npv - m0);
-            const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
-            for (int m = 0; m < mn; ++m) {
-              const float2 w = f2(__shfl_sync(FULLM, wl, m));
-              const float4 *row =
-                  reinterpret_cast<const float4 *>(img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + 4 * lane);
-              float4 a[QV];
-#pragma unroll
-              for (int c = 0; c < QV; ++c)
-                a[c] = (ub + 4 * lane + 128 * c < a1) ? LD::ld4(row + 32 * c) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-              for (int c = 0; c < QV; ++c) {
-                const float2 l2 = fma2(w, make_float2(a[c].x, a[c].y), make_float2(q[c].x, q[c].y));
-                const float2 h2 = fma2(w, make_float2(a[c].z, a[c].w), make_float2(q[c].z, q[c].w));
-                q[c] = make_float4(l2.x, l2.y, h2.x, h2.y);
-              }
-            }
-          }
-#pragma unroll
-          for (int c = 0; c < QV; ++c) {
-            const int u = ub + 4 * lane + 128 * c;
-            if (u < a1) *reinterpret_cast<float4 *>(Q + u) = q[c];
-          }
-        }
-      } else {
-      constexpr int QC = 16;
-      for (int ub = lo; ub < hi; ub += 32 * QC) {
-        float q[QC];
-#pragma unroll
-        for (int c = 0; c < QC; ++c) q[c] = 0.f;
-        for (int m0 = 0; m0 < npv; m0 += 32) {
-          const int mn = min(32, npv - m0);
-          const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
-          for (int m = 0; m < mn; ++m) {
-            const float w = __shfl_sync(FULLM, wl, m);
-            const float *row = img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + lane;
-            float a[QC];
-#pragma unroll
-            for (int c = 0; c < QC; ++c) a[c] = (ub + lane + 32 * c < hi) ? LD::ld(row + 32 * c) : 0.f;
-#pragma unroll
-            for (int c = 0; c < QC; ++c) q[c] = fmaf(w, a[c], q[c]);
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < QC; ++c)
-          if (ub + lane + 32 * c < hi) Q[ub + lane + 32 * c] = q[c];
-      }
-      }
-      __syncwarp();
-      // per-voxel gathers, two voxels per instruction
-#pragma unroll
-      for (int p = 0; p < KP; ++p) {
-        const int L = max(up[p].n0, up[p].n1);
-        if (L <= 0) continue;
-        float2 Fp = first_edge_prim2(up[p]);
-        float2 S = f2(0.f);
-        float2 lf = f2(1.0f);
-        for (int l = 0; l < L; ++l) {
-          const float2 F = cubic_prim2(fma2(lf, up[p].inc, up[p].start));
-          const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
-          const float q0 = (l < up[p].n0) ? Q[up[p].lo0 + l] : 0.0f;
-          const float q1 = (l < up[p].n1) ? Q[up[p].lo1 + l] : 0.0f;
-          S = fma2(w, make_float2(q0, q1), S);
-          Fp = F;
-          lf = add2(lf, f2(1.0f));
-        }
-        // Kahan (packed): acc += wgt * rho * S
-        const float2 term = mul2(mul2(up[p].rho, S), f2(wgt));
-        const float2 y = add2(term, make_float2(-cmp[p].x, -cmp[p].y));
-        const float2 t = add2(acc[p], y);
-        cmp[p] = add2(add2(t, make_float2(-acc[p].x, -acc[p].y)), make_float2(-y.x, -y.y));
-        acc[p] = t;
-      }
-      __syncwarp();
+      for (int p = 0; p < KP; ++p) kahan2(acc[p], cmp[p], mul2(term[p], f2(wgt)));
     }
   }
   float *dst = vol + (long)gate * gate_stride + (long)col * nz;
@@ -454,6 +481,85 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
     if (k0 < nz) dst[k0] += acc[p].x - cmp[p].x;
     if (k1 < nz) dst[k1] += acc[p].y - cmp[p].y;
   }
+}
+
+// Column item over all gates at once.  One warp: column col, voxels
+// kbase + lane + 64 p (+32), p < KP; every view of [view_lo, view_hi) once
+// (images at sino[view - view_lo]), its contribution added with weight
+// pairs[view].w0 into gate pairs[view].g0 and with w1 into g1 (g1 < 0:
+// none).  Per-gate sums with Kahan compensation live in this warp's shared
+// rows sacc / scmp ([ngates][64 KP] floats each; lane-private entries);
+// the result is added into vol (one owner per voxel and gate).
+template <int GEOM, int KP, class LD>
+__device__ __forceinline__ void column_item_gates(const Params3D &P, const View3D *__restrict__ views,
+                                                  const GatePair *__restrict__ pairs, int view_lo,
+                                                  int view_hi, const float *sino, long sino_view_stride,
+                                                  float *__restrict__ vol, long gate_stride, int ngates,
+                                                  int col, int kbase, float *Q, float *sacc, float *scmp,
+                                                  int *__restrict__ err, bool vec4 = false)
+{
+  const int lane = threadIdx.x & 31;
+  const int nz = P.nz;
+  const int i = col % P.nx, j = col / P.nx;
+  constexpr int W = 64 * KP;
+  for (int t = lane; t < ngates * W; t += 32) {
+    sacc[t] = 0.f;
+    scmp[t] = 0.f;
+  }
+  __syncwarp();
+  for (int vb = view_lo; vb < view_hi; vb += 32) {
+    const int myview = vb + lane;
+    ColGeo<MODEL_CUBIC> mine;
+    if (myview < view_hi) {
+      column_geo<GEOM, MODEL_CUBIC>(P, views[myview], i, j, 0, mine);
+      if (mine.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+    } else {
+      mine.vax.n = 0;
+      mine.bad = 1;
+    }
+    const int cnt = min(32, view_hi - vb);
+    for (int s = 0; s < cnt; ++s) {
+      const int nvx = __shfl_sync(FULLM, mine.vax.n, s);
+      const int bd = __shfl_sync(FULLM, mine.bad, s);
+      if (bd || nvx <= 0) continue;
+      const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
+      const int view = vb + s;
+      float2 term[KP];
+      if (!view_gather<GEOM, KP, LD>(P, views[view], cc, kbase,
+                                     sino + (long)(view - view_lo) * sino_view_stride, Q, vec4, term))
+        continue;
+      const GatePair gp = pairs[view];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int g = h ? gp.g1 : gp.g0;
+        const float wg = h ? gp.w1 : gp.w0;
+        if (g < 0) continue;
+        float *a = sacc + g * W, *c = scmp + g * W;
+#pragma unroll
+        for (int p = 0; p < KP; ++p) {
+          const int v0 = 64 * p + lane, v1 = v0 + 32;
+          float2 acc = make_float2(a[v0], a[v1]), cmp = make_float2(c[v0], c[v1]);
+          kahan2(acc, cmp, mul2(term[p], f2(wg)));
+          a[v0] = acc.x;
+          a[v1] = acc.y;
+          c[v0] = cmp.x;
+          c[v1] = cmp.y;
+        }
+      }
+    }
+  }
+  for (int g = 0; g < ngates; ++g) {
+    float *dst = vol + (long)g * gate_stride + (long)col * nz;
+    const float *a = sacc + g * W, *c = scmp + g * W;
+#pragma unroll
+    for (int p = 0; p < KP; ++p) {
+      const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
+      const int v0 = 64 * p + lane, v1 = v0 + 32;
+      if (k0 < nz) dst[k0] += a[v0] - c[v0];
+      if (k1 < nz) dst[k1] += a[v1] - c[v1];
+    }
+  }
+  __syncwarp();
 }
 
 }  // namespace trtt

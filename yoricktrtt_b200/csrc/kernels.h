@@ -21,6 +21,13 @@ struct GateEntry {
   float w;
 };
 
+// The transpose's gate weights of one view: w0 into gate g0, w1 into g1
+// (g1 < 0: none).  The same pairs as the per-gate entry lists, by view.
+struct GatePair {
+  int g0, g1;
+  float w0, w1;
+};
+
 struct Fwd3DLaunch {
   Params3D P;
   const View3D *views;   // device, nviews entries
@@ -49,6 +56,7 @@ struct Back3DLaunch {
   float *vol;            // column layout, accumulated
   long gate_stride;
   int factorized;        // 1: column kernel; 0: per-voxel kernel
+  const GatePair *pairs = nullptr;  // by view index; non-null: all gates in one pass over the views
   int *err;
 };
 
@@ -116,6 +124,12 @@ struct WlsLaunch {
 };
 size_t wls_smem(int nu, int band_rows);
 size_t band_fast_smem(int nu, int band_rows, int warps);
+// Floats of shared memory per warp of the all-gates transpose: the profile
+// row (nu, rounded up to 4) and the per-gate sums and compensations.
+__host__ __device__ inline size_t back_gates_row(int nu, int ngates, int kp)
+{
+  return (size_t)((nu + 3) & ~3) + 2 * (size_t)ngates * 64 * kp;
+}
 // Spread mode of the band item: row locks for voxel columns of 128 voxels
 // or more, shared atomics below (measured: 256^3 -> 512^2 83 -> 74 ms per
 // 360 views with locks; 128x128x64 -> 256^2 8.4 -> 9.9 ms, so atomics there).

@@ -358,6 +358,30 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
                                 blockIdx.y * (64 * KP), gate, sm + warp * P.nu, err, vec4 != 0);
 }
 
+// Transpose of a gated scan, all gates in one pass over the views: one warp
+// per (column, range of 64 KP voxels); each view's contribution goes to its
+// two gates (pairs[view]).  Shared memory per warp: the profile row and the
+// per-gate sums and compensations (back_gates_row floats).
+template <int GEOM, int KP>
+__global__ void __launch_bounds__(256)
+k_back3d_col_gates(const Params3D P, const View3D *__restrict__ views,
+                   const GatePair *__restrict__ pairs, int view_lo, int view_hi,
+                   const float *__restrict__ sino, long sino_view_stride, float *__restrict__ vol,
+                   long gate_stride, int ngates, int *__restrict__ err, int vec4)
+{
+  extern __shared__ __align__(16) float sm_g[];
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5;
+  const int ncols = P.nx * P.ny;
+  const int col = blockIdx.x * nwarps + warp;
+  if (col >= ncols) return;
+  float *row = sm_g + (size_t)warp * back_gates_row(P.nu, ngates, KP);
+  float *sacc = row + ((P.nu + 3) & ~3), *scmp = sacc + ngates * 64 * KP;
+  column_item_gates<GEOM, KP, LoadNC>(P, views, pairs, view_lo, view_hi, sino, sino_view_stride, vol,
+                                      gate_stride, ngates, col, blockIdx.y * (64 * KP), row, sacc, scmp,
+                                      err, vec4 != 0);
+}
+
 // ---------------------------------------------------------------------------
 // Launchers (cubic model, factorised views)
 // ---------------------------------------------------------------------------
@@ -403,23 +427,44 @@ static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
   return cudaGetLastError();
 }
 
-template <int GEOM>
-static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
+template <int GEOM, int KP>
+static cudaError_t back_fast_kp(const Back3DLaunch &L, cudaStream_t st)
 {
-  constexpr int KP = 4;  // 4 voxel pairs per lane: 256 voxels per warp-column pass
   const int warps = 8;
   const int ncols = L.P.nx * L.P.ny;
-  dim3 grid((ncols + warps - 1) / warps, (L.P.nz + 64 * KP - 1) / (64 * KP), L.ngates);
+  const int kblocks = (L.P.nz + 64 * KP - 1) / (64 * KP);
+  // 16-byte profile loads: rows of nu % 4 == 0 floats in 16-byte aligned images
+  const int vec4 = (L.P.nu % 4 == 0 && L.sino_view_stride % 4 == 0 &&
+                    ((uintptr_t)L.sino & 15) == 0) ? 1 : 0;
+  const size_t smem_gates = sizeof(float) * (size_t)warps * back_gates_row(L.P.nu, L.ngates, KP);
+  if (L.pairs && L.ngates > 1 && smem_gates <= 160u * 1024u) {
+    dim3 grid((ncols + warps - 1) / warps, kblocks);
+    auto kern = k_back3d_col_gates<GEOM, KP>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_gates);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, warps * 32, smem_gates, st>>>(L.P, L.views, L.pairs, L.view_lo, L.view_hi, L.sino,
+                                               L.sino_view_stride, L.vol, L.gate_stride, L.ngates,
+                                               L.err, vec4);
+    return cudaGetLastError();
+  }
+  dim3 grid((ncols + warps - 1) / warps, kblocks, L.ngates);
   const size_t smem = sizeof(float) * (size_t)warps * L.P.nu;
   auto kern = k_back3d_col_fast<GEOM, KP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  // 16-byte profile loads: rows of nu % 4 == 0 floats in 16-byte aligned images
-  const int vec4 = (L.P.nu % 4 == 0 && L.sino_view_stride % 4 == 0 &&
-                    ((uintptr_t)L.sino & 15) == 0) ? 1 : 0;
   kern<<<grid, warps * 32, smem, st>>>(L.P, L.views, L.gate_ptr, L.entries, L.view_lo, L.view_hi,
                                       L.sino, L.sino_view_stride, L.vol, L.gate_stride, L.err, vec4);
   return cudaGetLastError();
+}
+
+// Voxel pairs per lane by column length: 64 voxels (1), 128 (2), more (4),
+// so that short columns do not carry idle pairs.
+template <int GEOM>
+static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
+{
+  if (L.P.nz <= 64) return back_fast_kp<GEOM, 1>(L, st);
+  if (L.P.nz <= 128) return back_fast_kp<GEOM, 2>(L, st);
+  return back_fast_kp<GEOM, 4>(L, st);
 }
 
 cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
