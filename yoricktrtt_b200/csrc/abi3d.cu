@@ -343,6 +343,7 @@ extern "C" int trtt_b200_plan3d_wls_grad(trtt_b200_plan3d *pl, const float *vol,
   L.gate_ptr = pl->gate_ptr.as<int>();
   L.entries = pl->entries.as<GateEntry>();
   L.ngates = pl->nt;
+  L.pairs = pl->nt > 1 ? pl->pairs.as<GatePair>() : nullptr;
   L.vol = vol;
   L.gate_stride = (long)P.nx * P.ny * P.nz;
   L.y = y;

@@ -119,10 +119,12 @@ struct WlsLaunch {
   int extra_wait;            // column items also wait for this many band items (test hook)
   long long wait_ns;         // bound of that wait
   int *err;
+  const GatePair *pairs;      // by view; non-null with several gates: column items over all gates
   // filled by launch_wls_persistent
-  int nbands, kchunks, n_band_items, n_col_items, lock_spread;
+  int nbands, kchunks, n_band_items, n_col_items, lock_spread, gates_mode;
 };
 size_t wls_smem(int nu, int band_rows);
+size_t wls_gates_smem(int nu, int ngates, int kp, int gates_mode);
 size_t band_fast_smem(int nu, int band_rows, int warps);
 // Floats of shared memory per warp of the all-gates transpose: the profile
 // row (nu, rounded up to 4) and the per-gate sums and compensations.

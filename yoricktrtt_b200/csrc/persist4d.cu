@@ -16,9 +16,12 @@
 //                         projection of the band in shared memory, written
 //                         back as the weighted residual with the band's
 //                         FP64 cost;
-//   items [nb, nb + nc):  column items (gate, block of columns, k range):
-//                         the transpose gathered from the residuals of the
-//                         gate's views.
+//   items [nb, nb + nc):  column items (block of columns, k range): the
+//                         transpose gathered from the residuals, each view
+//                         once, into the view's two gates (with one gate, or
+//                         gates too many for shared memory: one item per
+//                         gate, block of columns and k range, over the
+//                         gate's views).
 // The uneven view counts of the gates need no padding: the queue holds
 // exactly one item per band and per column block.  A column item needs
 // every band item finished; a CTA that draws one waits on the count of
@@ -28,6 +31,8 @@
 // TRTT_ERR_STALL in the error word and returns.  The CTA that finishes
 // the last band item sums the band costs in item order (deterministic).
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "fast3d_items.cuh"
 #include "kernels.h"
@@ -136,16 +141,27 @@ k_wls_persistent(const WlsLaunch A)
       __syncthreads();
       if (!s_ok) break;
       const int ci = item - nb;
-      const int per_gate = colblocks * A.kchunks;
-      const int gate = ci / per_gate;
-      const int rem = ci - gate * per_gate;
-      const int cb = rem / A.kchunks, kc = rem - cb * A.kchunks;
-      const int col = cb * nwarps + warp;
-      if (col < ncols)
-        column_item<GEOM, KP, LoadCG>(P, A.views, A.entries, A.gate_ptr[gate], A.gate_ptr[gate + 1],
-                                      0, A.nviews, A.resid, (long)nu * nv, A.grad, A.gate_stride,
-                                      col, kc * (64 * KP), gate, sm + warp * nu, A.err,
-                                      (nu & 3) == 0);
+      if (A.gates_mode) {
+        const int cb = ci / A.kchunks, kc = ci - cb * A.kchunks;
+        const int col = cb * nwarps + warp;
+        float *row = sm + (size_t)warp * back_gates_row(nu, A.ngates, KP);
+        float *sacc = row + ((nu + 3) & ~3), *scmp = sacc + A.ngates * 64 * KP;
+        if (col < ncols)
+          column_item_gates<GEOM, KP, LoadCG>(P, A.views, A.pairs, 0, A.nviews, A.resid, (long)nu * nv,
+                                              A.grad, A.gate_stride, A.ngates, col, kc * (64 * KP), row,
+                                              sacc, scmp, A.err, (nu & 3) == 0);
+      } else {
+        const int per_gate = colblocks * A.kchunks;
+        const int gate = ci / per_gate;
+        const int rem = ci - gate * per_gate;
+        const int cb = rem / A.kchunks, kc = rem - cb * A.kchunks;
+        const int col = cb * nwarps + warp;
+        if (col < ncols)
+          column_item<GEOM, KP, LoadCG>(P, A.views, A.entries, A.gate_ptr[gate], A.gate_ptr[gate + 1],
+                                        0, A.nviews, A.resid, (long)nu * nv, A.grad, A.gate_stride,
+                                        col, kc * (64 * KP), gate, sm + warp * nu, A.err,
+                                        (nu & 3) == 0);
+      }
       __syncthreads();
     }
   }
@@ -155,7 +171,7 @@ template <int GEOM, int KP, int MINB>
 cudaError_t launch_wls(WlsLaunch L, int sms, cudaStream_t st)
 {
   auto kern = k_wls_persistent<GEOM, KP, MINB>;
-  const size_t smem = wls_smem(L.P.nu, L.band_rows);
+  const size_t smem = std::max(wls_smem(L.P.nu, L.band_rows), wls_gates_smem(L.P.nu, L.ngates, KP, L.gates_mode));
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -178,6 +194,13 @@ size_t wls_smem(int nu, int band_rows)
                           (size_t)band_rows);
 }
 
+// Shared memory of the column items over all gates: one profile row and
+// the per-gate sums of every warp (16 warps); 0 when not in that mode.
+size_t wls_gates_smem(int nu, int ngates, int kp, int gates_mode)
+{
+  return gates_mode ? sizeof(float) * 16 * back_gates_row(nu, ngates, kp) : 0;
+}
+
 int wls_kp(int nz)
 {
   return nz <= 64 ? 1 : (nz <= 128 ? 2 : 4);
@@ -190,7 +213,8 @@ cudaError_t launch_wls_persistent(WlsLaunch L, int sms, cudaStream_t st)
   L.nbands = (L.P.nv + L.band_rows - 1) / L.band_rows;
   L.n_band_items = L.nviews * L.nbands;
   L.lock_spread = band_lock_spread(L.P) ? 1 : 0;
-  L.n_col_items = L.ngates * ((L.P.nx * L.P.ny + 15) / 16) * L.kchunks;
+  L.gates_mode = (L.pairs && L.ngates > 1 && wls_gates_smem(L.P.nu, L.ngates, kp, 1) <= 200u * 1024u) ? 1 : 0;
+  L.n_col_items = (L.gates_mode ? 1 : L.ngates) * ((L.P.nx * L.P.ny + 15) / 16) * L.kchunks;
   const bool cone = L.P.geom == GEOM_CONE;
   // CTAs per SM: 1 (up to 128 registers per thread) or 2 (64)
   const bool two = L.ctas_per_sm == 2;
