@@ -520,15 +520,19 @@ int trtt_b200_cb3d_cubic_forward_noalloc(const float *vol_columns, float *sino,
  * unet_status: -1 if a convolution kernel gave up waiting for its tensor-core
  *   work (bounded waits), then clears the flag; synchronises the stream. */
 int trtt_b200_conv3_pack(const float *w, int cout, int cin, int transpose, void *wpack, void *stream);
-/* Staging of trtt_b200_conv3_forward, process-wide: 0 (default) copies each
- * stage's slab and weights into shared memory with 16-byte cp.async by all
- * 128 threads; 1 loads them with TMA (2D tiled copies of the padded
+/* Staging of trtt_b200_conv3_forward, process-wide: 0 copies each stage's
+ * slab and weights into shared memory with 16-byte cp.async by all 128
+ * threads; 1 loads them with TMA (2D tiled copies of the padded
  * channels-last activations, a bulk copy of the weights) issued by one
  * producer thread while one thread issues the MMAs on an mbarrier ring
- * (warp specialisation).  Both compute the same MMAs in the same order
- * (identical results).  TMA is the default when the driver provides a
- * tensor-map encoder (forward pass of the 128^3 U-Net 1.73 -> 1.37 ms);
- * on < 0 restores that default.  -1 when asked for TMA without one.  No counterpart in the reference. */
+ * (warp specialisation), one tile per CTA; 2 is the same in persistent
+ * CTAs of 6 warps that walk many tiles with two tensor-memory accumulators,
+ * the epilogue of one tile (4 warps) overlapping the copies and MMAs of the
+ * next (needs 2 x 2 x n <= 512 tensor-memory columns; else 1; measured
+ * slower than 1 on the 128^3 U-Net: 1.96 vs 1.37 ms per forward pass).  All
+ * compute the same MMAs in the same order (identical results).  Default
+ * (on < 0): 1 when the driver provides a tensor-map encoder, else 0.  -1
+ * when asked for TMA without one.  No counterpart in the reference. */
 int trtt_b200_conv3_set_tma(int on);
 int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, const void *wpack, int n,
                             const float *bias, int mode, float slope, void *y, void *y2, int n1,

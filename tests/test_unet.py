@@ -223,10 +223,12 @@ def test_unet_training_reduces_loss(lib):
                                            (64, 0, 64, (1, 4, 6, 130)), (32, 16, 96, (2, 6, 10, 20))])
 def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
     """TMA staging with a producer thread and an MMA thread on an mbarrier
-    ring (trtt_b200_conv3_set_tma(1)) gives the same outputs as the cp.async
-    staging: the same MMAs in the same order.  The widths cover a slab of
-    one partial TMA box (w = 20), of several boxes (w = 130: 518 rows, two
-    full boxes of 256 and one of 6)."""
+    ring, one tile per CTA (trtt_b200_conv3_set_tma(1)) or persistent CTAs
+    with two tensor-memory accumulators and epilogue warps (2), gives the
+    same outputs as the cp.async staging: the same MMAs in the same order.
+    The widths cover a slab of one partial TMA box (w = 20), of several
+    boxes (w = 130: 518 rows, two full boxes of 256 and one of 6); 96
+    output channels take the whole tensor memory (2 x 2 x 96 columns)."""
     from yoricktrtt_b200._lib import check
     from yoricktrtt_b200.unet import _p, _stream
     g = torch.Generator().manual_seed(c1 + 3 * c2 + co)
@@ -242,7 +244,7 @@ def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
     rows = xp1.shape[0]
     outs = []
     try:
-        for tma in (0, 1):
+        for tma in (0, 1, 2):
             check(lib.trtt_b200_conv3_set_tma(tma), "set_tma")
             y = torch.zeros(rows, co, dtype=torch.float32, device="cuda")
             check(lib.trtt_b200_conv3_forward(_p(xp1), c1, _p(xp2), c2, _p(pack), co, _p(bias), 1, 1.0,
@@ -254,8 +256,9 @@ def test_conv3_forward_tma_staging(lib, c1, c2, co, dims):
             outs.append((y.cpu(), yb.cpu()))
     finally:
         lib.trtt_b200_conv3_set_tma(-1)
-    assert torch.equal(outs[0][0], outs[1][0])
-    assert torch.equal(outs[0][1], outs[1][1])
+    for o in outs[1:]:
+        assert torch.equal(outs[0][0], o[0])
+        assert torch.equal(outs[0][1], o[1])
     ref = _conv_ref(torch.cat([x1, x2], 1) if c2 else x1, _bf(wt), bias.double().cpu())
     got = outs[1][0].reshape(nb, d + 2, h + 2, w + 2, co)[:, 1:-1, 1:-1, 1:-1].permute(0, 4, 1, 2, 3).double()
     assert rel_l2(got.numpy(), ref.numpy()) <= 1e-5
@@ -273,7 +276,7 @@ def test_unet_training_step_tma_staging():
     t = torch.rand(1, 32, 32, 32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(2))
     res = []
     try:
-        for tma in (0, 1):
+        for tma in (0, 1, 2):
             _lib.check(lib.trtt_b200_conv3_set_tma(tma), "set_tma")
             net = UNet3D(seed=3)
             y = net.forward(x).clone()
@@ -283,9 +286,10 @@ def test_unet_training_step_tma_staging():
                         {(k, n): g.clone().cpu() for k, v in net._grads.items() for n, g in v.items()}))
     finally:
         lib.trtt_b200_conv3_set_tma(-1)
-    assert torch.equal(res[0][0], res[1][0])
-    # the loss and the bias gradients are sums with float atomics: equal to
-    # FP32 summation order
-    assert abs(res[0][1] - res[1][1]) <= 1e-6 * abs(res[0][1])
-    for key, g0 in res[0][2].items():
-        assert rel_l2(res[1][2][key].double().numpy(), g0.double().numpy()) <= 1e-5, key
+    for r in res[1:]:
+        assert torch.equal(res[0][0], r[0])
+        # the loss and the bias gradients are sums with float atomics: equal
+        # to FP32 summation order
+        assert abs(res[0][1] - r[1]) <= 1e-6 * abs(res[0][1])
+        for key, g0 in res[0][2].items():
+            assert rel_l2(r[2][key].double().numpy(), g0.double().numpy()) <= 1e-5, key

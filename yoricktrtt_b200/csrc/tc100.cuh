@@ -161,6 +161,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *m, uint32_t byte
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)), "r"(bytes)
                : "memory");
 }
+// Plain arrive (count 1) on an mbarrier of this CTA.
+__device__ __forceinline__ void mbar_arrive(uint64_t *m)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(m)) : "memory");
+}
 // 2D tiled load of the tensor map's box at element coordinates (x, y), x
 // the innermost dimension (x * element size a multiple of 16 bytes).
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *tmap, int x, int y, uint64_t *mbar)

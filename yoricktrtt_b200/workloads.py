@@ -348,12 +348,13 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     return res
 
 
-def unet_case(size=128, batch=1, reps=1, train=1, tma=1, seed=0):
+def unet_case(size=128, batch=1, reps=1, train=1, tma=-1, seed=0):
     """One U-Net case for profiling the tensor-core convolutions: ``reps``
     forward passes (and training steps when ``train``) on a batch of
     size^3 inputs; returns the CUDA-event time of the last of each.
-    ``tma=0`` stages the forward / input-gradient convolutions with
-    cp.async instead of TMA."""
+    ``tma`` selects the staging of the forward / input-gradient
+    convolutions (trtt_b200_conv3_set_tma): 0 cp.async, 1 TMA one tile per
+    CTA, 2 TMA in persistent CTAs, -1 the default."""
     torch = _torch()
     from . import _lib
     from .unet import UNet3D
@@ -363,7 +364,7 @@ def unet_case(size=128, batch=1, reps=1, train=1, tma=1, seed=0):
     x = torch.rand(batch, size, size, size, device="cuda", generator=g)
     t = torch.rand(batch, size, size, size, device="cuda", generator=g)
     res = {"config": f"U-Net 3 levels 16/32/64, batch {batch} x {size}^3, "
-                     f"{'TMA' if tma else 'cp.async'} staging"}
+                     f"staging {({0: 'cp.async', 1: 'TMA per tile', 2: 'TMA persistent'}).get(int(tma), 'default')}"}
     for _ in range(reps):
         a, e = _events()
         a.record()
