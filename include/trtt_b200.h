@@ -528,10 +528,10 @@ int trtt_b200_conv3_pack(const float *w, int cout, int cin, int transpose, void 
  * (warp specialisation), one tile per CTA; 2 is the same in persistent
  * CTAs of 6 warps that walk many tiles with two tensor-memory accumulators,
  * the epilogue of one tile (4 warps) overlapping the copies and MMAs of the
- * next (needs 2 x 2 x n <= 512 tensor-memory columns; else 1; measured
- * slower than 1 on the 128^3 U-Net: 1.96 vs 1.37 ms per forward pass).  All
- * compute the same MMAs in the same order (identical results).  Default
- * (on < 0): 1 when the driver provides a tensor-map encoder, else 0.  -1
+ * next (needs 2 x 2 x n <= 512 tensor-memory columns; else 1).  All
+ * compute the same MMAs in the same order (identical results).  Forward
+ * pass of the 128^3 U-Net: 1.73 ms (0), 1.37 ms (1), 1.18 ms (2).  Default
+ * (on < 0): 2 when the driver provides a tensor-map encoder, else 0.  -1
  * when asked for TMA without one.  No counterpart in the reference. */
 int trtt_b200_conv3_set_tma(int on);
 int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, const void *wpack, int n,

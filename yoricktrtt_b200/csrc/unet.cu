@@ -1179,10 +1179,10 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   a.g = make_grid(nb, d, h, w);
   a.row0 = a.g.plane;
   // staging: 0 cp.async, 1 TMA per tile, 2 TMA persistent (two tensor-memory
-  // accumulators: 2 S n columns must fit in 512; measured slower than 1 on
-  // the 128^3 U-Net, 1.96 vs 1.37 ms per forward pass); automatic: TMA per
-  // tile when the driver can encode tensor maps, else cp.async
-  int tma = g_conv_tma < 0 ? (encode_tiled() ? 1 : 0) : g_conv_tma;
+  // accumulators: 2 S n columns must fit in 512); automatic: the persistent
+  // kernel where it applies, else TMA per tile, else cp.async (forward pass
+  // of the 128^3 U-Net: 1.18 / 1.37 / 1.73 ms)
+  int tma = g_conv_tma < 0 ? (encode_tiled() ? 2 : 0) : g_conv_tma;
   if (tma == 2 && pow2_cols(2 * S * n) > 512) tma = 1;
   if (tma) {
     FwdPlan pl = fwd_plan_tma(n, a.groups, a.g);
@@ -1218,6 +1218,12 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
       TRTT_CK(cudaGetDevice(&dev));
       TRTT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       TRTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3_fwd_pers<S>, 192, pl.smem));
+      // the query answered 1 where two CTAs fit (measured: 1.96 ms per
+      // forward pass of the 128^3 U-Net at one CTA per SM, 1.18 ms at two);
+      // CTAs per SM by shared memory (plus the static and reserved bytes)
+      // and tensor memory, which residency_smem keeps consistent
+      const int by_smem = (int)((227L * 1024) / ((long)pl.smem + 2048));
+      occ = std::max(occ, std::min(by_smem, (int)(512u / pl.tmem_cols)));
       if (occ < 1) return fail("conv3_forward: the persistent kernel does not fit on an SM");
       const long grid = std::min<long>(pl.tiles, (long)sms * occ);
       k_conv3_fwd_pers<S><<<(unsigned)grid, 192, pl.smem, st>>>(a, maps, pl.tiles);
