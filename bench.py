@@ -432,6 +432,23 @@ def run_b200(args):
                  "volume": "the phantom + 0.05 + U[0, 0.1): every voxel non-zero"}
         del xd
 
+    # the same pair with the tabulated footprint (10 001 samples of the cubic
+    # B-spline primitive, the reference's size_footprint): the table model
+    # keeps the per-view kernels, whose table slots must be the reference's
+    table_model = None
+    if not args.skip_dense:
+        from yoricktrtt_b200 import footprint as F
+        from yoricktrtt_b200.projectors import Projector3D
+        prt = Projector3D(sc, F.make_footprint(3, 10001))
+        tsteps = 1
+        tms, tfwd, tback, _ = timed_pairs(prt, x, sino, back, flush, tsteps, 1, world, barrier)
+        tms = max_over_ranks(tms)
+        table_model = {"value": 2 * VIEWS * world * tsteps / (tms / 1e3), "unit": "projections/s",
+                       "fwd_ms": statistics.mean(tfwd), "back_ms": statistics.mean(tback),
+                       "steps": tsteps, "footprint": "table of 10001 samples (FP64), per-view kernels",
+                       "kernels": "k_fwd3d_band + k_back3d_col_fast (table model)"}
+        prt.close()
+
     # roofline of the dominant kernel: algorithmic bytes per launch (per-view
     # streaming model: the forward reads the volume and writes one detector
     # image per view, the transpose reads one image and writes the volume
@@ -508,6 +525,7 @@ def run_b200(args):
                                        "used": bool(grouped)}},
             "parity": parity,
             "dense": dense,
+            "table_model": table_model,
             "per_view_kernels": per_view,
             "roofline": {"bound": "issue", "kernel": kern, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

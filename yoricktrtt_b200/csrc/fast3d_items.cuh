@@ -289,6 +289,42 @@ struct LoadCG {
   __device__ __forceinline__ static float4 ld4(const float4 *p) { return __ldcg(p); }
 };
 
+// Column state of lane `src`, for either footprint model.
+template <int MODEL>
+__device__ __forceinline__ ColGeo<MODEL> shfl_colm(const ColGeo<MODEL> &c, int src)
+{
+  if constexpr (MODEL == MODEL_CUBIC) {
+    return shfl_colc(c, src);
+  } else {
+    ColGeo<MODEL> r;
+    r.vax.lo = __shfl_sync(FULLM, c.vax.lo, src);
+    r.vax.n = __shfl_sync(FULLM, c.vax.n, src);
+    r.vax.start = __shfl_sync(FULLM, c.vax.start, src);
+    r.vax.inc = __shfl_sync(FULLM, c.vax.inc, src);
+    r.bad = 0;
+    r.q = __shfl_sync(FULLM, c.q, src);
+    r.magn = __shfl_sync(FULLM, c.magn, src);
+    r.delta_v = __shfl_sync(FULLM, c.delta_v, src);
+    r.vca8sqr = __shfl_sync(FULLM, c.vca8sqr, src);
+    r.nyj = __shfl_sync(FULLM, c.nyj, src);
+    r.nxi = __shfl_sync(FULLM, c.nxi, src);
+    return r;
+  }
+}
+
+// Per-voxel u-footprints of a lane's voxels k0, k1 (either model): the
+// closed form evaluates both with packed FP32 (UPair); the table model
+// keeps the reference's exact FP64 axes (voxel_u), so that every table slot
+// is the reference's own.
+template <int MODEL> struct VoxPair;
+template <> struct VoxPair<MODEL_CUBIC> {
+  UPair up;
+};
+template <> struct VoxPair<MODEL_TABLE> {
+  AxisTable ax0, ax1;
+  float rho0, rho1;
+};
+
 // One view's contribution to the voxels kbase + lane + 64 p (+32), p < KP,
 // of column (i, j): term[p] = rho * sum_u w(u) Q[u] for the lane's two
 // voxels, with Q[u] = sum_v wv(v) img[v][u] the column's v-collapsed profile
@@ -296,29 +332,41 @@ struct LoadCG {
 // the column's geometry in the view.  Returns false (term untouched, Q not
 // used) when the footprints of the warp's voxels miss the detector.  vec4:
 // nu % 4 == 0 and 16-byte aligned images (16-byte loads).  All lanes call it.
-template <int GEOM, int KP, class LD>
+template <int GEOM, int KP, class LD, int MODEL = MODEL_CUBIC>
 __device__ __forceinline__ bool view_gather(const Params3D &P, const View3D &V,
-                                            const ColGeo<MODEL_CUBIC> &cc, int kbase,
+                                            const ColGeo<MODEL> &cc, int kbase,
                                             const float *img0, float *Q, bool vec4,
                                             float2 (&term)[KP])
 {
   const int lane = threadIdx.x & 31;
   const int nu = P.nu, nz = P.nz;
-  UPair up[KP];
+  VoxPair<MODEL> vp[KP];
   int lo = INT_MAX, hi = INT_MIN;
 #pragma unroll
   for (int p = 0; p < KP; ++p) {
     const int k0 = kbase + lane + 64 * p, k1 = k0 + 32;
-    voxel_u_pair<GEOM>(P, V, cc, k0, k1, up[p]);
-    if (k0 >= nz) up[p].n0 = 0;
-    if (k1 >= nz) up[p].n1 = 0;
-    if (up[p].n0 > 0) {
-      lo = min(lo, up[p].lo0);
-      hi = max(hi, up[p].lo0 + up[p].n0);
+    int lo0 = 0, n0 = 0, lo1 = 0, n1 = 0;
+    if constexpr (MODEL == MODEL_CUBIC) {
+      UPair &up = vp[p].up;
+      voxel_u_pair<GEOM>(P, V, cc, k0, k1, up);
+      if (k0 >= nz) up.n0 = 0;
+      if (k1 >= nz) up.n1 = 0;
+      lo0 = up.lo0; n0 = up.n0; lo1 = up.lo1; n1 = up.n1;
+    } else {
+      VoxPair<MODEL_TABLE> &t = vp[p];
+      t.ax0.n = 0;
+      t.ax1.n = 0;
+      if (!(k0 < nz && voxel_u<GEOM, MODEL_TABLE>(P, V, cc, k0, t.ax0, t.rho0))) t.ax0.n = 0;
+      if (!(k1 < nz && voxel_u<GEOM, MODEL_TABLE>(P, V, cc, k1, t.ax1, t.rho1))) t.ax1.n = 0;
+      lo0 = t.ax0.lo; n0 = t.ax0.n; lo1 = t.ax1.lo; n1 = t.ax1.n;
     }
-    if (up[p].n1 > 0) {
-      lo = min(lo, up[p].lo1);
-      hi = max(hi, up[p].lo1 + up[p].n1);
+    if (n0 > 0) {
+      lo = min(lo, lo0);
+      hi = max(hi, lo0 + n0);
+    }
+    if (n1 > 0) {
+      lo = min(lo, lo1);
+      hi = max(hi, lo1 + n1);
     }
   }
   lo = __reduce_min_sync(FULLM, lo);
@@ -339,7 +387,7 @@ __device__ __forceinline__ bool view_gather(const Params3D &P, const View3D &V,
       for (int c = 0; c < QV; ++c) q[c] = make_float4(0.f, 0.f, 0.f, 0.f);
       for (int m0 = 0; m0 < npv; m0 += 32) {
         const int mn = min(32, npv - m0);
-        const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+        const float wl = (lane < mn) ? axis_weight<MODEL>(cc.vax, m0 + lane, P) : 0.f;
         for (int m = 0; m < mn; ++m) {
           const float2 w = f2(__shfl_sync(FULLM, wl, m));
           const float4 *row =
@@ -370,7 +418,7 @@ __device__ __forceinline__ bool view_gather(const Params3D &P, const View3D &V,
       for (int c = 0; c < QC; ++c) q[c] = 0.f;
       for (int m0 = 0; m0 < npv; m0 += 32) {
         const int mn = min(32, npv - m0);
-        const float wl = (lane < mn) ? axis_weight<MODEL_CUBIC>(cc.vax, m0 + lane, P) : 0.f;
+        const float wl = (lane < mn) ? axis_weight<MODEL>(cc.vax, m0 + lane, P) : 0.f;
         for (int m = 0; m < mn; ++m) {
           const float w = __shfl_sync(FULLM, wl, m);
           const float *row = img0 + (long)(cc.vax.lo + m0 + m) * nu + ub + lane;
@@ -387,25 +435,50 @@ __device__ __forceinline__ bool view_gather(const Params3D &P, const View3D &V,
     }
   }
   __syncwarp();
-  // per-voxel gathers, two voxels per instruction
+  // per-voxel gathers
 #pragma unroll
   for (int p = 0; p < KP; ++p) {
     term[p] = f2(0.f);
-    const int L = max(up[p].n0, up[p].n1);
-    if (L <= 0) continue;
-    float2 Fp = first_edge_prim2(up[p]);
-    float2 S = f2(0.f);
-    float2 lf = f2(1.0f);
-    for (int l = 0; l < L; ++l) {
-      const float2 F = cubic_prim2(fma2(lf, up[p].inc, up[p].start));
-      const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
-      const float q0 = (l < up[p].n0) ? Q[up[p].lo0 + l] : 0.0f;
-      const float q1 = (l < up[p].n1) ? Q[up[p].lo1 + l] : 0.0f;
-      S = fma2(w, make_float2(q0, q1), S);
-      Fp = F;
-      lf = add2(lf, f2(1.0f));
+    if constexpr (MODEL == MODEL_CUBIC) {
+      // two voxels per instruction
+      const UPair &up = vp[p].up;
+      const int L = max(up.n0, up.n1);
+      if (L <= 0) continue;
+      float2 Fp = first_edge_prim2(up);
+      float2 S = f2(0.f);
+      float2 lf = f2(1.0f);
+      for (int l = 0; l < L; ++l) {
+        const float2 F = cubic_prim2(fma2(lf, up.inc, up.start));
+        const float2 w = add2(F, make_float2(-Fp.x, -Fp.y));
+        const float q0 = (l < up.n0) ? Q[up.lo0 + l] : 0.0f;
+        const float q1 = (l < up.n1) ? Q[up.lo1 + l] : 0.0f;
+        S = fma2(w, make_float2(q0, q1), S);
+        Fp = F;
+        lf = add2(lf, f2(1.0f));
+      }
+      term[p] = mul2(up.rho, S);
+    } else {
+      // table edges in FP64 at the reference's positions (edge_table)
+      const VoxPair<MODEL_TABLE> &t = vp[p];
+      float s0 = 0.f, s1 = 0.f;
+      if (t.ax0.n > 0) {
+        double p0 = edge_table(t.ax0, 0, P.cum, P.last);
+        for (int l = 0; l < t.ax0.n; ++l) {
+          const double p1 = edge_table(t.ax0, l + 1, P.cum, P.last);
+          s0 = fmaf((float)(p1 - p0), Q[t.ax0.lo + l], s0);
+          p0 = p1;
+        }
+      }
+      if (t.ax1.n > 0) {
+        double p0 = edge_table(t.ax1, 0, P.cum, P.last);
+        for (int l = 0; l < t.ax1.n; ++l) {
+          const double p1 = edge_table(t.ax1, l + 1, P.cum, P.last);
+          s1 = fmaf((float)(p1 - p0), Q[t.ax1.lo + l], s1);
+          p0 = p1;
+        }
+      }
+      term[p] = make_float2(t.rho0 * s0, t.rho1 * s1);
     }
-    term[p] = mul2(up[p].rho, S);
   }
   __syncwarp();  // Q is free for the next view
   return true;
@@ -426,7 +499,7 @@ __device__ __forceinline__ void kahan2(float2 &acc, float2 &cmp, float2 term)
 // warp's nu floats.  vec4: nu % 4 == 0 and 16-byte aligned images (the
 // profile is then built from 16-byte loads).  Adds the result into vol (one
 // owner per voxel).
-template <int GEOM, int KP, class LD>
+template <int GEOM, int KP, class LD, int MODEL = MODEL_CUBIC>
 __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__restrict__ views,
                                             const GateEntry *__restrict__ entries, int e0, int e1,
                                             int view_lo, int view_hi, const float *sino,
@@ -445,14 +518,14 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
   }
   for (int eb = e0; eb < e1; eb += 32) {
     const int me = eb + lane;
-    ColGeo<MODEL_CUBIC> mine;
+    ColGeo<MODEL> mine;
     int myview = 0;
     float myw = 0.f;
     const GateEntry ge = (me < e1) ? entries[me] : GateEntry{-1, 0.f};
     if (ge.view >= view_lo && ge.view < view_hi) {
       myview = ge.view;
       myw = ge.w;
-      column_geo<GEOM, MODEL_CUBIC>(P, views[myview], i, j, 0, mine);
+      column_geo<GEOM, MODEL>(P, views[myview], i, j, 0, mine);
       if (mine.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
     } else {
       mine.vax.n = 0;
@@ -463,11 +536,11 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
       const int nvx = __shfl_sync(FULLM, mine.vax.n, s);
       const int bd = __shfl_sync(FULLM, mine.bad, s);
       if (bd || nvx <= 0) continue;
-      const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
+      const ColGeo<MODEL> cc = shfl_colm<MODEL>(mine, s);
       const int view = __shfl_sync(FULLM, myview, s);
       const float wgt = __shfl_sync(FULLM, myw, s);
       float2 term[KP];
-      if (!view_gather<GEOM, KP, LD>(P, views[view], cc, kbase,
+      if (!view_gather<GEOM, KP, LD, MODEL>(P, views[view], cc, kbase,
                                      sino + (long)(view - view_lo) * sino_view_stride, Q, vec4, term))
         continue;
 #pragma unroll
@@ -490,7 +563,7 @@ __device__ __forceinline__ void column_item(const Params3D &P, const View3D *__r
 // none).  Per-gate sums with Kahan compensation live in this warp's shared
 // rows sacc / scmp ([ngates][64 KP] floats each; lane-private entries);
 // the result is added into vol (one owner per voxel and gate).
-template <int GEOM, int KP, class LD>
+template <int GEOM, int KP, class LD, int MODEL = MODEL_CUBIC>
 __device__ __forceinline__ void column_item_gates(const Params3D &P, const View3D *__restrict__ views,
                                                   const GatePair *__restrict__ pairs, int view_lo,
                                                   int view_hi, const float *sino, long sino_view_stride,
@@ -509,9 +582,9 @@ __device__ __forceinline__ void column_item_gates(const Params3D &P, const View3
   __syncwarp();
   for (int vb = view_lo; vb < view_hi; vb += 32) {
     const int myview = vb + lane;
-    ColGeo<MODEL_CUBIC> mine;
+    ColGeo<MODEL> mine;
     if (myview < view_hi) {
-      column_geo<GEOM, MODEL_CUBIC>(P, views[myview], i, j, 0, mine);
+      column_geo<GEOM, MODEL>(P, views[myview], i, j, 0, mine);
       if (mine.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
     } else {
       mine.vax.n = 0;
@@ -522,10 +595,10 @@ __device__ __forceinline__ void column_item_gates(const Params3D &P, const View3
       const int nvx = __shfl_sync(FULLM, mine.vax.n, s);
       const int bd = __shfl_sync(FULLM, mine.bad, s);
       if (bd || nvx <= 0) continue;
-      const ColGeo<MODEL_CUBIC> cc = shfl_colc(mine, s);
+      const ColGeo<MODEL> cc = shfl_colm<MODEL>(mine, s);
       const int view = vb + s;
       float2 term[KP];
-      if (!view_gather<GEOM, KP, LD>(P, views[view], cc, kbase,
+      if (!view_gather<GEOM, KP, LD, MODEL>(P, views[view], cc, kbase,
                                      sino + (long)(view - view_lo) * sino_view_stride, Q, vec4, term))
         continue;
       const GatePair gp = pairs[view];

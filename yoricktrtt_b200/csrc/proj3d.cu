@@ -479,7 +479,9 @@ cudaError_t launch_fwd3d(const Fwd3DLaunch &L, cudaStream_t st)
 
 cudaError_t launch_back3d(const Back3DLaunch &L, cudaStream_t st)
 {
-  if (L.P.model == MODEL_CUBIC && L.factorized) return launch_back3d_fast(L, st);
+  // factorised views: the column kernels of proj3d_fast.cu (both models;
+  // the table model with its exact FP64 per-voxel axes)
+  if (L.factorized) return launch_back3d_fast(L, st);
   if (L.P.geom == GEOM_CONE)
     return L.P.model == MODEL_TABLE ? launch_back<GEOM_CONE, MODEL_TABLE>(L, st)
                                     : launch_back<GEOM_CONE, MODEL_CUBIC>(L, st);

@@ -338,7 +338,7 @@ k_fwd3d_pull(const Params3D P, const View3D *__restrict__ views,
 // ---------------------------------------------------------------------------
 // Transpose
 // ---------------------------------------------------------------------------
-template <int GEOM, int KP>
+template <int GEOM, int KP, int MODEL>
 __global__ void __launch_bounds__(256)
 k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
                   const int *__restrict__ gate_ptr, const GateEntry *__restrict__ entries,
@@ -353,7 +353,7 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
   const int col = blockIdx.x * nwarps + warp;
   if (col >= ncols) return;
   const int gate = blockIdx.z;
-  column_item<GEOM, KP, LoadNC>(P, views, entries, gate_ptr[gate], gate_ptr[gate + 1], view_lo,
+  column_item<GEOM, KP, LoadNC, MODEL>(P, views, entries, gate_ptr[gate], gate_ptr[gate + 1], view_lo,
                                 view_hi, sino, sino_view_stride, vol, gate_stride, col,
                                 blockIdx.y * (64 * KP), gate, sm + warp * P.nu, err, vec4 != 0);
 }
@@ -362,7 +362,7 @@ k_back3d_col_fast(const Params3D P, const View3D *__restrict__ views,
 // per (column, range of 64 KP voxels); each view's contribution goes to its
 // two gates (pairs[view]).  Shared memory per warp: the profile row and the
 // per-gate sums and compensations (back_gates_row floats).
-template <int GEOM, int KP>
+template <int GEOM, int KP, int MODEL>
 __global__ void __launch_bounds__(256)
 k_back3d_col_gates(const Params3D P, const View3D *__restrict__ views,
                    const GatePair *__restrict__ pairs, int view_lo, int view_hi,
@@ -377,7 +377,7 @@ k_back3d_col_gates(const Params3D P, const View3D *__restrict__ views,
   if (col >= ncols) return;
   float *row = sm_g + (size_t)warp * back_gates_row(P.nu, ngates, KP);
   float *sacc = row + ((P.nu + 3) & ~3), *scmp = sacc + ngates * 64 * KP;
-  column_item_gates<GEOM, KP, LoadNC>(P, views, pairs, view_lo, view_hi, sino, sino_view_stride, vol,
+  column_item_gates<GEOM, KP, LoadNC, MODEL>(P, views, pairs, view_lo, view_hi, sino, sino_view_stride, vol,
                                       gate_stride, ngates, col, blockIdx.y * (64 * KP), row, sacc, scmp,
                                       err, vec4 != 0);
 }
@@ -427,7 +427,7 @@ static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
   return cudaGetLastError();
 }
 
-template <int GEOM, int KP>
+template <int GEOM, int KP, int MODEL>
 static cudaError_t back_fast_kp(const Back3DLaunch &L, cudaStream_t st)
 {
   const int warps = 8;
@@ -439,7 +439,7 @@ static cudaError_t back_fast_kp(const Back3DLaunch &L, cudaStream_t st)
   const size_t smem_gates = sizeof(float) * (size_t)warps * back_gates_row(L.P.nu, L.ngates, KP);
   if (L.pairs && L.ngates > 1 && smem_gates <= 160u * 1024u) {
     dim3 grid((ncols + warps - 1) / warps, kblocks);
-    auto kern = k_back3d_col_gates<GEOM, KP>;
+    auto kern = k_back3d_col_gates<GEOM, KP, MODEL>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_gates);
     if (e != cudaSuccess) return e;
     kern<<<grid, warps * 32, smem_gates, st>>>(L.P, L.views, L.pairs, L.view_lo, L.view_hi, L.sino,
@@ -449,7 +449,7 @@ static cudaError_t back_fast_kp(const Back3DLaunch &L, cudaStream_t st)
   }
   dim3 grid((ncols + warps - 1) / warps, kblocks, L.ngates);
   const size_t smem = sizeof(float) * (size_t)warps * L.P.nu;
-  auto kern = k_back3d_col_fast<GEOM, KP>;
+  auto kern = k_back3d_col_fast<GEOM, KP, MODEL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<grid, warps * 32, smem, st>>>(L.P, L.views, L.gate_ptr, L.entries, L.view_lo, L.view_hi,
@@ -457,14 +457,15 @@ static cudaError_t back_fast_kp(const Back3DLaunch &L, cudaStream_t st)
   return cudaGetLastError();
 }
 
-// Voxel pairs per lane by column length: 64 voxels (1), 128 (2), more (4),
-// so that short columns do not carry idle pairs.
-template <int GEOM>
+// Voxel pairs per lane by column length: 64 voxels (1), 128 (2), more (4;
+// the table model, whose per-voxel axes are FP64, at most 2), so that short
+// columns do not carry idle pairs.
+template <int GEOM, int MODEL>
 static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
 {
-  if (L.P.nz <= 64) return back_fast_kp<GEOM, 1>(L, st);
-  if (L.P.nz <= 128) return back_fast_kp<GEOM, 2>(L, st);
-  return back_fast_kp<GEOM, 4>(L, st);
+  if (L.P.nz <= 64) return back_fast_kp<GEOM, 1, MODEL>(L, st);
+  if (L.P.nz <= 128 || MODEL == MODEL_TABLE) return back_fast_kp<GEOM, 2, MODEL>(L, st);
+  return back_fast_kp<GEOM, MODEL == MODEL_TABLE ? 2 : 4, MODEL>(L, st);
 }
 
 cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
@@ -475,7 +476,11 @@ cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
 
 cudaError_t launch_back3d_fast(const Back3DLaunch &L, cudaStream_t st)
 {
-  return L.P.geom == GEOM_CONE ? back_fast<GEOM_CONE>(L, st) : back_fast<GEOM_PARALLEL>(L, st);
+  if (L.P.model == MODEL_TABLE)
+    return L.P.geom == GEOM_CONE ? back_fast<GEOM_CONE, MODEL_TABLE>(L, st)
+                                 : back_fast<GEOM_PARALLEL, MODEL_TABLE>(L, st);
+  return L.P.geom == GEOM_CONE ? back_fast<GEOM_CONE, MODEL_CUBIC>(L, st)
+                               : back_fast<GEOM_PARALLEL, MODEL_CUBIC>(L, st);
 }
 
 size_t band_fast_smem(int nu, int band_rows, int warps)

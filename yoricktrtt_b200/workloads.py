@@ -300,7 +300,7 @@ def learned_eval(weights=None, n_test=20, eval_maxiter=500, ref_maxiter=600, see
 
 
 def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps=1, dense=0,
-                   tiles=None, sym=2, gshape=None, seed=0):
+                   tiles=None, sym=2, gshape=None, table=0, seed=0):
     """One cone-beam projector case for profiling: an n x n x nz volume of 20
     ellipsoids (``dense=1`` adds a positive floor so that every voxel is
     non-zero), ``views`` views on an nd x nd detector, SID 1000 mm, SDD
@@ -308,16 +308,18 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     direct and/or transpose launches, checks the status flag and returns the
     CUDA-event time of the last launch of each direction.  ``tiles`` is a
     set_tiles() argument list; ``sym=0`` bypasses the group kernels, ``sym=1``
-    selects per-member profiles; ``gshape`` is a set_group_shape() list."""
+    selects per-member profiles; ``gshape`` is a set_group_shape() list;
+    ``table > 0`` uses the tabulated cubic footprint with that many samples
+    (the table model runs the per-view kernels)."""
     torch = _torch()
-    from . import geometry as G, phantoms as P
+    from . import footprint as F, geometry as G, phantoms as P
     from .projectors import Projector3D, columns_from_xyz
     nz = nz or n
     sc = G.circular_scan_3d(n, n, nz, 1.0, 3, nd, nd, 1.0, 1.0, views, rsc=1000.0, rsd=1500.0)
     vol = P.ellipsoids_3d(n, n, nz, n=20, seed=seed, dtype=np.float32)
     if dense:
         vol = vol + np.float32(0.05)
-    pr = Projector3D(sc)
+    pr = Projector3D(sc, F.make_footprint(3, int(table)) if table else None)
     if tiles:
         pr.set_tiles(*tiles)
     pr.set_symmetry(int(sym))
@@ -326,7 +328,8 @@ def projector_case(n=128, nd=256, views=90, nz=None, direct=1, transpose=1, reps
     x = columns_from_xyz(torch.tensor(vol, device="cuda"))
     y = torch.zeros(pr.detector_shape(), device="cuda")
     b = torch.zeros_like(x)
-    res = {"config": f"cone {n}x{n}x{nz} -> {views} x {nd}^2, cubic, {'dense' if dense else 'phantom'}",
+    model = f"cubic table of {int(table)} samples" if table else "cubic"
+    res = {"config": f"cone {n}x{n}x{nz} -> {views} x {nd}^2, {model}, {'dense' if dense else 'phantom'}",
            "groups": pr.groups(), "symmetry": int(sym), "gshape": gshape}
     for _ in range(reps):
         if direct:
