@@ -446,7 +446,7 @@ def run_b200(args):
         table_model = {"value": 2 * VIEWS * world * tsteps / (tms / 1e3), "unit": "projections/s",
                        "fwd_ms": statistics.mean(tfwd), "back_ms": statistics.mean(tback),
                        "steps": tsteps, "footprint": "table of 10001 samples (FP64), per-view kernels",
-                       "kernels": "k_fwd3d_band + k_back3d_col_fast (table model)"}
+                       "kernels": "k_fwd3d_band_table + k_back3d_col_fast (table model)"}
         prt.close()
 
     # roofline of the dominant kernel: algorithmic bytes per launch (per-view

@@ -45,6 +45,7 @@ CASES = [
     ("CB3D", G.TRTT_CONE_BEAM, dict(us=0.7, vs=1.3, s=0.8)),     # anisotropic
     ("CB3D", G.TRTT_CONE_BEAM, dict(u_off=3.3, v_off=-2.1)),     # detector offsets
     ("PB3D", G.TRTT_PARALLEL_BEAM, dict(nu=22, nv=18, us=0.6, vs=0.6)),
+    ("CB3D", G.TRTT_CONE_BEAM, dict(nu=20, nv=18, us=1.8, vs=1.8)),  # coarse cells: non-monotone columns
 ]
 
 

@@ -22,6 +22,7 @@
 namespace trtt {
 
 static constexpr int SPREAD_CHUNKS = 16;  // footprints up to 512 cells wide spread from registers
+static constexpr int TABLE_LMAX = 10;     // table model: footprints up to 10 cells from registers
 
 // True when floor(uc_k - hs_k), the first cell of voxel k's u-footprint
 // before any clamp, strictly increases or decreases along the column: the
@@ -29,9 +30,9 @@ static constexpr int SPREAD_CHUNKS = 16;  // footprints up to 512 cells wide spr
 // offset l, so a warp can update its profile with plain loads and stores.
 // |d uc/dk| = |B|; hs = hs0 h_u0 magn delta_u varies by at most
 // hs0 h_u0m |B| max|uc - a12| u_scl^2 inv_den per voxel.
-template <int GEOM>
+template <int GEOM, int MODEL = MODEL_CUBIC>
 __device__ __forceinline__ bool column_monotone(const Params3D &P, const View3D &V,
-                                                const ColGeo<MODEL_CUBIC> &c)
+                                                const ColGeo<MODEL> &c)
 {
   const double b = fabs(c.B);
   if constexpr (GEOM == GEOM_CONE) {
@@ -87,6 +88,70 @@ __device__ __forceinline__ void row_unlock(int *lock)
   }
 }
 
+
+// Spread of a warp's column profile over the band: acc[rb - v0 + r][u] +=
+// wv[r] * prof[u] for the nr rows r and the cells [lo, hi) (lo, hi: the
+// lane's own range, reduced here over the warp); the profile is cleared on
+// the way.  Modes as in band_item.  All lanes call it.
+__device__ __forceinline__ void band_spread(int lo, int hi, int rb, int v0, int nr, int nu,
+                                            float *acc, float *prof, const float *wv, int *locks,
+                                            int *__restrict__ err, bool lock_spread)
+{
+  const int lane = threadIdx.x & 31;
+  lo = __reduce_min_sync(FULLM, lo);
+  hi = __reduce_max_sync(FULLM, hi);
+  __syncwarp();
+  if (lo < hi && hi - lo <= 32 * SPREAD_CHUNKS) {
+    // profile read once into registers (and cleared), then the rows
+    // one at a time
+    float pv[SPREAD_CHUNKS];
+#pragma unroll
+    for (int q = 0; q < SPREAD_CHUNKS; ++q) {
+      const int u = lo + lane + 32 * q;
+      pv[q] = 0.f;
+      if (u < hi) {
+        pv[q] = prof[u];
+        prof[u] = 0.f;
+      }
+    }
+    for (int r = 0; r < nr; ++r) {
+      const float w = wv[r];
+      const int row = rb - v0 + r;
+      float *rowp = acc + row * nu;
+      if (lock_spread) {
+        if (!row_lock(locks + row, err)) continue;
+#pragma unroll
+        for (int q = 0; q < SPREAD_CHUNKS; ++q) {
+          const int u = lo + lane + 32 * q;
+          if (u < hi) rowp[u] = fmaf(w, pv[q], rowp[u]);
+        }
+        row_unlock(locks + row);
+      } else {
+#pragma unroll
+        for (int q = 0; q < SPREAD_CHUNKS; ++q) {
+          const int u = lo + lane + 32 * q;
+          if (u < hi) atomicAdd(rowp + u, w * pv[q]);
+        }
+      }
+    }
+  } else if (lo < hi) {
+    for (int r = 0; r < nr; ++r) {
+      const float w = wv[r];
+      const int row = rb - v0 + r;
+      float *rowp = acc + row * nu;
+      if (lock_spread) {
+        if (!row_lock(locks + row, err)) continue;
+        for (int u = lo + lane; u < hi; u += 32) rowp[u] = fmaf(w, prof[u], rowp[u]);
+        row_unlock(locks + row);
+      } else {
+        for (int u = lo + lane; u < hi; u += 32) atomicAdd(rowp + u, w * prof[u]);
+      }
+    }
+    __syncwarp();
+    for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;
+  }
+  __syncwarp();
+}
 
 // Band item.  acc: band_rows x nu floats (zeroed by the caller), prof: this
 // warp's nu-float profile (zero on entry and on exit), wv: this warp's
@@ -220,59 +285,7 @@ __device__ __forceinline__ void band_item(const Params3D &P, const View3D &V,
           }
         }
       }
-      lo = __reduce_min_sync(FULLM, lo);
-      hi = __reduce_max_sync(FULLM, hi);
-      __syncwarp();
-      if (lo < hi && hi - lo <= 32 * SPREAD_CHUNKS) {
-        // profile read once into registers (and cleared), then the rows
-        // one at a time
-        float pv[SPREAD_CHUNKS];
-#pragma unroll
-        for (int q = 0; q < SPREAD_CHUNKS; ++q) {
-          const int u = lo + lane + 32 * q;
-          pv[q] = 0.f;
-          if (u < hi) {
-            pv[q] = prof[u];
-            prof[u] = 0.f;
-          }
-        }
-        for (int r = 0; r < nr; ++r) {
-          const float w = wv[r];
-          const int row = rb - v0 + r;
-          float *rowp = acc + row * nu;
-          if (lock_spread) {
-            if (!row_lock(locks + row, err)) continue;
-#pragma unroll
-            for (int q = 0; q < SPREAD_CHUNKS; ++q) {
-              const int u = lo + lane + 32 * q;
-              if (u < hi) rowp[u] = fmaf(w, pv[q], rowp[u]);
-            }
-            row_unlock(locks + row);
-          } else {
-#pragma unroll
-            for (int q = 0; q < SPREAD_CHUNKS; ++q) {
-              const int u = lo + lane + 32 * q;
-              if (u < hi) atomicAdd(rowp + u, w * pv[q]);
-            }
-          }
-        }
-      } else if (lo < hi) {
-        for (int r = 0; r < nr; ++r) {
-          const float w = wv[r];
-          const int row = rb - v0 + r;
-          float *rowp = acc + row * nu;
-          if (lock_spread) {
-            if (!row_lock(locks + row, err)) continue;
-            for (int u = lo + lane; u < hi; u += 32) rowp[u] = fmaf(w, prof[u], rowp[u]);
-            row_unlock(locks + row);
-          } else {
-            for (int u = lo + lane; u < hi; u += 32) atomicAdd(rowp + u, w * prof[u]);
-          }
-        }
-        __syncwarp();
-        for (int u = lo + lane; u < hi; u += 32) prof[u] = 0.f;
-      }
-      __syncwarp();
+      band_spread(lo, hi, rb, v0, nr, nu, acc, prof, wv, locks, err, lock_spread);
     }
   }
 }
@@ -324,6 +337,110 @@ template <> struct VoxPair<MODEL_TABLE> {
   AxisTable ax0, ax1;
   float rho0, rho1;
 };
+
+// Band item of the table model (direct, column-factorised views): the
+// decomposition of band_item with the reference's exact FP64 per-voxel
+// axes (voxel_u<GEOM, MODEL_TABLE>) and FP64 table edges, so every table
+// slot is the reference's own.  Lane j takes voxel kb + j of a warp step
+// (FP64 axes leave nothing to pack).  Profile: on a monotone column
+// (column_monotone) the 32 voxels of a step have distinct first cells
+// unless a first cell was clamped to the detector's first or last cell, so
+// a step without such a cell writes distinct cells at every footprint
+// offset and updates the profile with plain loads and stores (offsets
+// ordered by __syncwarp); other steps use shared atomics.  Footprints of
+// up to TABLE_LMAX cells load their edges together into registers first.
+// Spread: band_spread.  Same arguments and contract as band_item.
+template <int GEOM>
+__device__ __forceinline__ void band_item_table(const Params3D &P, const View3D &V,
+                                                const float *__restrict__ vol, long gate_stride,
+                                                int v0, int v1, float *acc, float *prof, float *wv,
+                                                int *locks, int *s_next, int *__restrict__ err,
+                                                bool lock_spread)
+{
+  const int lane = threadIdx.x & 31;
+  const int nu = P.nu, nz = P.nz;
+  const int ncols = P.nx * P.ny;
+  const int nchunks = (ncols + 31) >> 5;
+  const double *__restrict__ cum = P.cum;
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(s_next, 1);
+    chunk = __shfl_sync(FULLM, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int mycol = (chunk << 5) + lane;
+    ColGeo<MODEL_TABLE> c;
+    bool hit = false;
+    int my_mono = 0;
+    if (mycol < ncols) {
+      column_geo<GEOM, MODEL_TABLE>(P, V, mycol % P.nx, mycol / P.nx, 0, c);
+      if (c.bad) atomicOr(err, TRTT_ERR_SOURCE_PLANE);
+      hit = !c.bad && c.vax.n > 0 && c.vax.lo + c.vax.n > v0 && c.vax.lo < v1;
+      if (hit) my_mono = column_monotone<GEOM, MODEL_TABLE>(P, V, c) ? 1 : 0;
+    }
+    unsigned mask = __ballot_sync(FULLM, hit);
+    while (mask) {
+      const int src = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const ColGeo<MODEL_TABLE> cc = shfl_colm<MODEL_TABLE>(c, src);
+      const bool mono = __shfl_sync(FULLM, my_mono, src) != 0;
+      const int col = (chunk << 5) + src;
+      const int vl = cc.vax.lo, vr = cc.vax.lo + cc.vax.n;
+      const int rb = max(vl, v0), re = min(vr, v1), nr = re - rb;
+      for (int r = lane; r < nr; r += 32) wv[r] = axis_weight<MODEL_TABLE>(cc.vax, rb - vl + r, P);
+      int lo = INT_MAX, hi = INT_MIN;
+      const long cbase = (long)col * nz;
+      for (int kb = 0; kb < nz; kb += 32) {
+        const int k = kb + lane;
+        const float x = (k < nz) ? vox_val(vol, gate_stride, V, cbase + k) : 0.0f;
+        if (!__any_sync(FULLM, x != 0.0f)) continue;
+        AxisTable ax{};
+        float rho0 = 0.f;
+        int n = 0;
+        if (x != 0.0f && voxel_u<GEOM, MODEL_TABLE>(P, V, cc, k, ax, rho0)) n = ax.n;
+        const float xr = x * rho0;
+        const bool edge = n > 0 && (ax.lo == 0 || ax.lo == nu - 1);
+        const int Lw = __reduce_max_sync(FULLM, n);
+        if (Lw <= TABLE_LMAX) {
+          // the footprint's weights first: its n + 1 table edges are
+          // independent loads, issued together
+          float w[TABLE_LMAX];
+          {
+            double e[TABLE_LMAX + 1];
+#pragma unroll
+            for (int l = 0; l <= TABLE_LMAX; ++l) e[l] = (l <= n) ? edge_table(ax, l, cum, P.last) : 0.0;
+#pragma unroll
+            for (int l = 0; l < TABLE_LMAX; ++l) w[l] = (float)(e[l + 1] - e[l]) * xr;
+          }
+          if (mono && !__any_sync(FULLM, edge)) {
+#pragma unroll
+            for (int l = 0; l < TABLE_LMAX; ++l) {
+              if (l < Lw) {
+                if (l < n) prof[ax.lo + l] += w[l];
+                __syncwarp();
+              }
+            }
+          } else {
+#pragma unroll
+            for (int l = 0; l < TABLE_LMAX; ++l)
+              if (l < n) atomicAdd(prof + ax.lo + l, w[l]);
+          }
+        } else {
+          double p0 = n > 0 ? edge_table(ax, 0, cum, P.last) : 0.0;
+          for (int l = 0; l < n; ++l) {
+            const double p1 = edge_table(ax, l + 1, cum, P.last);
+            atomicAdd(prof + ax.lo + l, (float)(p1 - p0) * xr);
+            p0 = p1;
+          }
+        }
+        if (n > 0) {
+          lo = min(lo, ax.lo);
+          hi = max(hi, ax.lo + n);
+        }
+      }
+      band_spread(lo, hi, rb, v0, nr, nu, acc, prof, wv, locks, err, lock_spread);
+    }
+  }
+}
 
 // One view's contribution to the voxels kbase + lane + 64 p (+32), p < KP,
 // of column (i, j): term[p] = rho * sum_u w(u) Q[u] for the lane's two

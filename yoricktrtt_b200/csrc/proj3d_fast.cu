@@ -20,11 +20,13 @@ namespace trtt {
 // ---------------------------------------------------------------------------
 // Direct projector
 // ---------------------------------------------------------------------------
-template <int GEOM>
-__global__ void __launch_bounds__(512)
-k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
-                  const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
-                  long sino_view_stride, int band_rows, int *__restrict__ err, int lock_spread)
+// One CTA: detector rows [v0, v1) of view blockIdx.y, band in shared memory
+// (band item of the model), written back once.
+template <int GEOM, int MODEL>
+__device__ __forceinline__ void band_cta(const Params3D &P, const View3D *__restrict__ views,
+                                         const float *__restrict__ vol, long gate_stride,
+                                         float *__restrict__ sino, long sino_view_stride,
+                                         int band_rows, int *__restrict__ err, int lock_spread)
 {
   extern __shared__ float sm[];
   __shared__ View3D sV;
@@ -47,8 +49,12 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
   for (int t = threadIdx.x; t < band_rows; t += blockDim.x) locks[t] = 0;
   for (int t = lane; t < nu; t += 32) prof[t] = 0.f;
   __syncthreads();
-  band_item<GEOM>(P, sV, vol, gate_stride, v0, v1, band_rows, acc, prof, wv, locks, &s_next, err,
-                  lock_spread != 0);
+  if constexpr (MODEL == MODEL_TABLE)
+    band_item_table<GEOM>(P, sV, vol, gate_stride, v0, v1, acc, prof, wv, locks, &s_next, err,
+                          lock_spread != 0);
+  else
+    band_item<GEOM>(P, sV, vol, gate_stride, v0, v1, band_rows, acc, prof, wv, locks, &s_next, err,
+                    lock_spread != 0);
   __syncthreads();
   float *out = sino + (long)vi * sino_view_stride;
   const int nrow = v1 - v0;
@@ -56,6 +62,27 @@ k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
     const int r = t / nu, u = t - r * nu;
     out[(long)(v0 + r) * nu + u] += acc[t];
   }
+}
+
+template <int GEOM>
+__global__ void __launch_bounds__(512)
+k_fwd3d_band_fast(const Params3D P, const View3D *__restrict__ views,
+                  const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
+                  long sino_view_stride, int band_rows, int *__restrict__ err, int lock_spread)
+{
+  band_cta<GEOM, MODEL_CUBIC>(P, views, vol, gate_stride, sino, sino_view_stride, band_rows, err,
+                              lock_spread);
+}
+
+// Table model: the FP64 per-voxel axes; MINB CTAs per SM (register budget).
+template <int GEOM, int MINB>
+__global__ void __launch_bounds__(512, MINB)
+k_fwd3d_band_table(const Params3D P, const View3D *__restrict__ views,
+                   const float *__restrict__ vol, long gate_stride, float *__restrict__ sino,
+                   long sino_view_stride, int band_rows, int *__restrict__ err, int lock_spread)
+{
+  band_cta<GEOM, MODEL_TABLE>(P, views, vol, gate_stride, sino, sino_view_stride, band_rows, err,
+                              lock_spread);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,9 +425,35 @@ static cudaError_t fwd_pull(const Fwd3DLaunch &L, cudaStream_t st)
   return cudaGetLastError();
 }
 
+template <int GEOM, int MODEL, int MINB = 1>
+static cudaError_t fwd_band(const Fwd3DLaunch &L, cudaStream_t st)
+{
+  dim3 grid((L.P.nv + L.band_rows - 1) / L.band_rows, L.nviews);
+  const size_t smem = band_fast_smem(L.P.nu, L.band_rows, L.warps);
+  auto kern = MODEL == MODEL_TABLE ? k_fwd3d_band_table<GEOM, MINB> : k_fwd3d_band_fast<GEOM>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, L.warps * 32, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino,
+                                        L.sino_view_stride, L.band_rows, L.err,
+                                        band_lock_spread(L.P) ? 1 : 0);
+  return cudaGetLastError();
+}
+
 template <int GEOM>
 static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
 {
+  if (L.P.model == MODEL_TABLE) {
+    // Two 16-warp CTAs per SM (64 registers per thread) only where their
+    // shared memory leaves the cumulative table (read through L1 at random
+    // slots) room in the SM's 256 KB of L1 and shared memory; else one
+    // (up to 128 registers).  With the table evicted from L1 every edge
+    // lookup goes to L2.
+    const size_t smem = band_fast_smem(L.P.nu, L.band_rows, L.warps);
+    const size_t table = sizeof(double) * (size_t)L.P.size + 16u * 1024u;
+    const bool two = L.warps == 16 && 2 * (smem + 1024) <= 228u * 1024u &&
+                     2 * (smem + 1024) + table <= 256u * 1024u;
+    return two ? fwd_band<GEOM, MODEL_TABLE, 2>(L, st) : fwd_band<GEOM, MODEL_TABLE, 1>(L, st);
+  }
   if (L.pull) {
     if (L.P.nu <= 128) return fwd_pull<GEOM, 4>(L, st);
     if (L.P.nu <= 256) return fwd_pull<GEOM, 8>(L, st);
@@ -417,14 +470,7 @@ static cudaError_t fwd_fast(const Fwd3DLaunch &L, cudaStream_t st)
                                           L.sino_view_stride, L.band_rows, L.err);
     return cudaGetLastError();
   }
-  const size_t smem = band_fast_smem(L.P.nu, L.band_rows, L.warps);
-  auto kern = k_fwd3d_band_fast<GEOM>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  kern<<<grid, L.warps * 32, smem, st>>>(L.P, L.views, L.vol, L.gate_stride, L.sino,
-                                        L.sino_view_stride, L.band_rows, L.err,
-                                        band_lock_spread(L.P) ? 1 : 0);
-  return cudaGetLastError();
+  return fwd_band<GEOM, MODEL_CUBIC>(L, st);
 }
 
 template <int GEOM, int KP, int MODEL>
@@ -470,7 +516,7 @@ static cudaError_t back_fast(const Back3DLaunch &L, cudaStream_t st)
 
 cudaError_t launch_fwd3d_fast(const Fwd3DLaunch &L, cudaStream_t st)
 {
-  if (L.tc) return launch_fwd3d_tc(L, st);
+  if (L.tc && L.P.model == MODEL_CUBIC) return launch_fwd3d_tc(L, st);
   return L.P.geom == GEOM_CONE ? fwd_fast<GEOM_CONE>(L, st) : fwd_fast<GEOM_PARALLEL>(L, st);
 }
 
