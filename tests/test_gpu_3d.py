@@ -196,16 +196,20 @@ def test_view_subrange_and_tiles(oracle_port):
     assert rel_l2(a, ref) <= TOL
 
 
-def test_empty_and_offdetector(oracle_port):
+@pytest.mark.parametrize("model", ["cubic", "table"])
+@pytest.mark.parametrize("off", [(400.0, -300.0), (-30.0, 12.0)])
+def test_empty_and_offdetector(oracle_port, model, off):
     # detector shifted far away: every footprint is clipped to nothing or
-    # to the last cells, exactly as the reference clamps
-    sc = _scan(G.TRTT_CONE_BEAM, views=2, u_off=400.0, v_off=-300.0)
+    # to the last cells, exactly as the reference clamps; shifted by part of
+    # its width: many footprints start left of the first cell (clamped)
+    sc = _scan(G.TRTT_CONE_BEAM, views=2, u_off=off[0], v_off=off[1])
+    table = TABLE if model == "table" else None
     vol = _vol(sc)
     for v in range(2):
         ref = np.zeros((sc.nv, sc.nu))
         got = np.zeros_like(ref)
-        oracle_port.cb3d(ref, vol, sc, v, 0)
-        dropin.scan3d_call("CB3D", got, vol, sc, v, 0)
+        assert oracle_port._p3d("CB3D", ref, vol, sc, v, 0, table) == 0
+        dropin.scan3d_call("CB3D", got, vol, sc, v, 0, table)
         assert np.allclose(got, ref, rtol=1e-5, atol=1e-9 * max(1.0, np.abs(ref).max()))
 
 
