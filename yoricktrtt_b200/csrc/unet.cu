@@ -1026,28 +1026,28 @@ struct FwdPlan {
   uint32_t tmem_cols;
 };
 
-FwdPlan fwd_plan(int n, int groups, const Grid3 &g)
+FwdPlan fwd_plan(int n, int groups, const Grid3 &g, int S = kFwdS)
 {
   FwdPlan p;
-  p.rh = 128 * kFwdS + 2 * g.wp + 2;
+  p.rh = 128 * S + 2 * g.wp + 2;
   p.cs = ((p.rh * 16 + 127) / 128) * 128 + 64;
   p.stage_bytes = ((2 * p.cs + 288 * n + 1023) / 1024) * 1024;
   // a tile with at most 3 stages (16 input channels) has all of them in
   // flight from the start: 3 buffers, and one more CTA per SM
   p.nstg = (3 * groups <= 3 || 4 * p.stage_bytes > 112 * 1024) ? 3 : 4;
-  p.tmem_cols = pow2_cols(kFwdS * n);
+  p.tmem_cols = pow2_cols(S * n);
   p.smem = residency_smem(p.nstg * p.stage_bytes, p.tmem_cols);
   const long span = g.rows - 2 * g.plane;
-  p.tiles = (span + 128 * kFwdS - 1) / (128 * kFwdS);
+  p.tiles = (span + 128 * S - 1) / (128 * S);
   return p;
 }
 
 // Stage layout of the TMA forward kernel: as fwd_plan with the chunk stride
 // a multiple of 128 bytes (TMA writes shared memory at 128-byte-aligned
 // addresses).
-FwdPlan fwd_plan_tma(int n, int groups, const Grid3 &g)
+FwdPlan fwd_plan_tma(int n, int groups, const Grid3 &g, int S = kFwdS)
 {
-  FwdPlan p = fwd_plan(n, groups, g);
+  FwdPlan p = fwd_plan(n, groups, g, S);
   p.cs = ((p.rh * 16 + 127) / 128) * 128;
   p.stage_bytes = ((2 * p.cs + 288 * n + 1023) / 1024) * 1024;
   p.nstg = (3 * groups <= 3 || 4 * p.stage_bytes > 112 * 1024) ? 3 : 4;
@@ -1184,10 +1184,21 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   // of the 128^3 U-Net: 1.18 / 1.37 / 1.73 ms)
   int tma = g_conv_tma < 0 ? (encode_tiled() ? 2 : 0) : g_conv_tma;
   if (tma == 2 && pow2_cols(2 * S * n) > 512) tma = 1;
+  // persistent tiles of 4 x 128 rows where two CTAs still fit on an SM
+  // (tensor memory 2 x 4 n columns <= 256, and shared memory): the slab of a
+  // tile overlaps the next tile's by 2 (w+2) + 2 rows, so longer tiles stage
+  // each input row fewer times (1.5 instead of 2 slab rows per output row
+  // at 128^3) and fetch each stage's weights for twice the rows
+  bool s4 = false;
+  if (tma == 2 && pow2_cols(2 * 4 * n) <= 256) {
+    FwdPlan p4 = fwd_plan_tma(n, a.groups, a.g, 4);
+    p4.nstg = 4 * p4.stage_bytes <= 112 * 1024 ? 4 : 3;
+    s4 = 2 * ((long)residency_smem(p4.nstg * p4.stage_bytes, pow2_cols(2 * 4 * n)) + 2048) <= 227L * 1024;
+  }
   if (tma) {
-    FwdPlan pl = fwd_plan_tma(n, a.groups, a.g);
+    FwdPlan pl = fwd_plan_tma(n, a.groups, a.g, s4 ? 4 : S);
     if (tma == 2) {
-      pl.tmem_cols = pow2_cols(2 * S * n);
+      pl.tmem_cols = pow2_cols(2 * (s4 ? 4 : S) * n);
       pl.nstg = 4 * pl.stage_bytes <= 112 * 1024 ? 4 : 3;
       pl.smem = residency_smem(pl.nstg * pl.stage_bytes, pl.tmem_cols);
     }
@@ -1210,14 +1221,15 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
     if (!ok) return fail("conv3_forward: tensor map encoding failed");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (tma == 2) {
-      TRTT_CK(set_smem(k_conv3_fwd_pers<S>, pl.smem));
+      auto kern = s4 ? k_conv3_fwd_pers<4> : k_conv3_fwd_pers<S>;
+      TRTT_CK(set_smem(kern, pl.smem));
       // all of the SM's unified memory as shared memory, so that the
       // occupancy below (and the launch) can hold several CTAs
-      TRTT_CK(cudaFuncSetAttribute(k_conv3_fwd_pers<S>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      TRTT_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
       int dev = 0, sms = 0, occ = 0;
       TRTT_CK(cudaGetDevice(&dev));
       TRTT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      TRTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv3_fwd_pers<S>, 192, pl.smem));
+      TRTT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 192, pl.smem));
       // the query answered 1 where two CTAs fit (measured: 1.96 ms per
       // forward pass of the 128^3 U-Net at one CTA per SM, 1.18 ms at two);
       // CTAs per SM by shared memory (plus the static and reserved bytes)
@@ -1226,7 +1238,7 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
       occ = std::max(occ, std::min(by_smem, (int)(512u / pl.tmem_cols)));
       if (occ < 1) return fail("conv3_forward: the persistent kernel does not fit on an SM");
       const long grid = std::min<long>(pl.tiles, (long)sms * occ);
-      k_conv3_fwd_pers<S><<<(unsigned)grid, 192, pl.smem, st>>>(a, maps, pl.tiles);
+      kern<<<(unsigned)grid, 192, pl.smem, st>>>(a, maps, pl.tiles);
     } else {
       TRTT_CK(set_smem(k_conv3_fwd_tma<S>, pl.smem));
       k_conv3_fwd_tma<S><<<(unsigned)pl.tiles, 128, pl.smem, st>>>(a, maps);
