@@ -68,10 +68,20 @@ def test_conv3_forward(lib, c1, c2, co):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tma", [-1, 0])
 @pytest.mark.parametrize("c1,c2,co", [(16, 0, 16), (32, 16, 16), (64, 32, 32), (32, 0, 64)])
-def test_conv3_gradients(lib, c1, c2, co):
+def test_conv3_gradients(lib, c1, c2, co, tma):
     """Input gradient (transposed-flipped weights, split into the two input
-    tensors, accumulate) and weight/bias gradients against autograd."""
+    tensors, accumulate) and weight/bias gradients against autograd, with
+    the default TMA staging and with cp.async staging (set_tma(0))."""
+    try:
+        lib.trtt_b200_conv3_set_tma(tma)
+        _conv3_gradients(lib, c1, c2, co)
+    finally:
+        lib.trtt_b200_conv3_set_tma(-1)
+
+
+def _conv3_gradients(lib, c1, c2, co):
     from yoricktrtt_b200._lib import check
     from yoricktrtt_b200.unet import _p, _stream
     g = torch.Generator().manual_seed(7 * co + c1)

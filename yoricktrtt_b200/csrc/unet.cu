@@ -718,6 +718,165 @@ __global__ void __launch_bounds__(128) k_conv3_wgrad(const WgradArgs a)
   }
 }
 
+// Weight gradient with TMA staging.  The GEMM, the operand layouts (chunk
+// columns of 16-byte rows at strides csa / csb, all A regions ahead of the B
+// regions) and the MMAs are those of k_conv3_wgrad, in the same order; only
+// the staging differs.  Warp specialisation on an mbarrier ring:
+//   thread 0: producer.  For each stage it loads the dY rows (A: cout/8
+//     chunks of KT rows) and the input rows (B: cin/8 chunks of KT + 2 rows
+//     from x1 or x2) as 2D boxes of 8 channels x 128 rows (and a 2-row tail
+//     box) of the padded channels-last tensors (tensor maps of this GPU's
+//     own buffers, no multicast), completing on the buffer's `full`
+//     mbarrier as transaction bytes; it reuses a buffer after its `empty`
+//     barrier;
+//   thread 32: MMA issuer.  It waits on `full`, issues the stage's MMAs and
+//     commits them to `empty`; after the last stage it commits to `finb`;
+//   all four warps: the epilogue, after `finb`.
+// Rows outside a tensor read as zeros (the halo before its first row).  dY
+// rows at or past r1 belong to the last z border plane, zero by the layout,
+// or lie past the tensor.  Every wait is bounded (2 s); on a timeout the CTA
+// waits (bounded) for the copies it issued, sets the error word, frees its
+// tensor memory and leaves its partial sums unwritten.
+struct WgradMaps {
+  CUtensorMap dy, x1, x2;          // 8 channels x 128 rows
+  CUtensorMap x1_tail, x2_tail;    // 8 channels x 2 rows
+};
+
+__global__ void __launch_bounds__(128) k_conv3_wgrad_tma(const WgradArgs a, const __grid_constant__ WgradMaps maps)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[4], empty[4], finb;
+  __shared__ uint32_t s_taddr;
+  __shared__ volatile int s_bad;
+  __shared__ int s_issued, s_consumed;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gidx = blockIdx.x, dzi = gidx / 3, dyi = gidx - 3 * (gidx / 3);
+  const long off = (long)(dzi - 1) * a.g.plane + (long)(dyi - 1) * a.g.wp;
+  const int KT = a.kt;
+  const long qbeg = a.r0 + (long)blockIdx.y * a.steps * KT;
+  const long rem = a.r1 - qbeg;
+  int T = rem <= 0 ? 0 : (int)((rem + KT - 1) / KT);
+  if (T > a.steps) T = a.steps;
+  const int nstg = a.nstg, cin = a.cin;
+  const int nca = a.cout / 8, ncb = cin / 8;
+  const uint32_t sbase = tc::smem_addr(smem);
+  const uint32_t stage_tx = (uint32_t)(16 * (nca * KT + ncb * (KT + 2)));
+
+  if (tid == 0) {
+    for (int i = 0; i < nstg; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    tc::mbar_init(&finb, 1);
+    s_bad = 0;
+    s_issued = 0;
+    s_consumed = 0;
+    tc::mbar_fence_init();
+  }
+  // Only the cout/8 real chunks of A are staged; the M = 64 MMAs read the
+  // rows above cout from whatever follows them (see k_conv3_wgrad).
+  if (warp == 0) tc::tmem_alloc(&s_taddr, a.tmem_cols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = s_taddr;
+
+  if (tid == 0) {
+    // producer
+    int it = 0;
+    for (; it < T; ++it) {
+      const int slot = it % nstg;
+      if (it >= nstg && !tc::mbar_wait(&empty[slot], (uint32_t)((it / nstg) - 1) & 1u, kWaitNs)) {
+        s_bad = 1;
+        break;
+      }
+      if (s_bad) break;
+      const long q0 = qbeg + (long)it * KT;
+      const long hb = q0 + off - 1;
+      const uint32_t as = sbase + (uint32_t)(slot * a.a_bytes);
+      const uint32_t bs = sbase + (uint32_t)(nstg * a.a_bytes + slot * a.b_bytes);
+      tc::mbar_arrive_expect_tx(&full[slot], stage_tx);
+      for (int c = 0; c < nca; ++c)
+        for (int r0 = 0; r0 < KT; r0 += 128)
+          tc::tma_load_2d(as + (uint32_t)(c * a.csa + r0 * 16), &maps.dy, 8 * c, (int)(q0 + r0), &full[slot]);
+      for (int c = 0; c < ncb; ++c) {
+        const int ch = 8 * c;
+        const bool first = ch < a.c1;
+        const CUtensorMap *mb = first ? &maps.x1 : &maps.x2;
+        const CUtensorMap *mt = first ? &maps.x1_tail : &maps.x2_tail;
+        const int x = first ? ch : ch - a.c1;
+        for (int r0 = 0; r0 < KT; r0 += 128)
+          tc::tma_load_2d(bs + (uint32_t)(c * a.csb + r0 * 16), mb, x, (int)(hb + r0), &full[slot]);
+        tc::tma_load_2d(bs + (uint32_t)(c * a.csb + KT * 16), mt, x, (int)(hb + KT), &full[slot]);
+      }
+    }
+    s_issued = it;
+  } else if (tid == 32) {
+    // MMA issuer: the MMAs of k_conv3_wgrad, in the same order
+    const uint32_t idesc = tc::idesc_bf16(64, cin, 1, 1);
+    int it = 0;
+    for (; it < T; ++it) {
+      const int slot = it % nstg;
+      if (s_bad || !tc::mbar_wait(&full[slot], (uint32_t)(it / nstg) & 1u, kWaitNs)) {
+        s_bad = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t as = sbase + (uint32_t)(slot * a.a_bytes);
+      const uint32_t bs = sbase + (uint32_t)(nstg * a.a_bytes + slot * a.b_bytes);
+#pragma unroll 4
+      for (int ks = 0; ks < KT / 16; ++ks) {
+        const uint64_t ad = tc::sdesc(as + (uint32_t)(ks * 256), 128u, (uint32_t)a.csa);
+        for (int j = 0; j < 3; ++j) {
+          const uint64_t bd = tc::sdesc(bs + (uint32_t)((ks * 16 + j) * 16), 128u, (uint32_t)a.csb);
+          tc::mma_bf16(tmem + (uint32_t)(j * cin), ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&empty[slot]);
+    }
+    s_consumed = it;
+    tc::mma_commit(&finb);  // arrives once every MMA issued above has completed
+  }
+  const bool fin_ok = tc::mbar_wait(&finb, 0, kWaitNs);
+  __syncthreads();
+  const bool bad = s_bad || !fin_ok;
+  if (!bad) {
+    tc::fence_after_sync();
+    // M = 64 accumulator: row co = 16 q + r sits in tensor-memory lane 32 q + r
+    const int co = 16 * warp + lane;
+    const bool mine = lane < 16 && co < a.cout;
+    float *dst = a.part + ((long)blockIdx.y * a.cout + (mine ? co : 0)) * 27 * cin;
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+      const int tap = gidx * 3 + j;
+#pragma unroll 1
+      for (int c0 = 0; c0 < cin; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * cin + c0), v);
+        if (mine) {
+          float4 *o = reinterpret_cast<float4 *>(dst + (long)tap * cin + c0);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (T > 0) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            else o[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    // copies issued for stages the MMAs never consumed
+    for (int it = s_consumed; it < s_issued; ++it)
+      tc::mbar_wait(&full[it % nstg], (uint32_t)(it / nstg) & 1u, kWaitNs);
+    atomicExch(&g_unet_err, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, a.tmem_cols);
+  }
+}
+
 __global__ void k_sum_parts(const float *__restrict__ part, int chunks, long n, float *__restrict__ out)
 {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -1103,12 +1262,15 @@ struct WgradPlan {
   uint32_t tmem_cols;
 };
 
-WgradPlan wgrad_plan(int cout, int cin, const Grid3 &g)
+WgradPlan wgrad_plan(int cout, int cin, const Grid3 &g, bool tma = false)
 {
   WgradPlan p;
   const int nca = cout / 8, ncb = cin / 8;
-  const int pad_a = nca == 2 ? 64 : nca == 4 ? 32 : 16;
-  const int pad_b = ncb == 2 ? 64 : ncb == 4 ? 32 : 16;
+  // cp.async: chunk strides padded so that the threads' 16-byte writes of
+  // one row spread over the banks; TMA: strides of whole 128-byte lines
+  // (its shared-memory destinations are 128-byte aligned)
+  const int pad_a = tma ? 0 : nca == 2 ? 64 : nca == 4 ? 32 : 16;
+  const int pad_b = tma ? 0 : ncb == 2 ? 64 : ncb == 4 ? 32 : 16;
   p.tmem_cols = pow2_cols(3 * cin);
   for (int kt = 256; kt >= 128; kt /= 2) {
     p.kt = kt;
@@ -1300,8 +1462,10 @@ int trtt_b200_conv3_plan_info(int which, int cin, int cout, int nb, int d, int h
 size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w)
 {
   if (!grid_ok(nb, d, h, w) || cout <= 0 || cin <= 0 || cout % 8 || cin % 8) return 0;
-  WgradPlan p = wgrad_plan(cout, cin, make_grid(nb, d, h, w));
-  return (size_t)p.chunks * cout * 27 * cin * sizeof(float);
+  // enough for either staging
+  const Grid3 g = make_grid(nb, d, h, w);
+  const long chunks = std::max(wgrad_plan(cout, cin, g, false).chunks, wgrad_plan(cout, cin, g, true).chunks);
+  return (size_t)chunks * cout * 27 * cin * sizeof(float);
 }
 
 int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2, float *dw,
@@ -1324,7 +1488,13 @@ int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, cons
   a.g = make_grid(nb, d, h, w);
   a.r0 = a.g.plane;
   a.r1 = a.g.rows - a.g.plane;
-  const WgradPlan pl = wgrad_plan(cout, cin, a.g);
+  // staging: TMA unless cp.async is asked for (trtt_b200_conv3_set_tma(0)) or
+  // the driver has no tensor-map encoder; rows must be addressable by the
+  // 32-bit coordinates of a tensor copy, the tensors 16-byte aligned
+  const bool tma = g_conv_tma != 0 && encode_tiled() && a.g.rows + 512 < 0x7FFFFFFFL &&
+                   !(reinterpret_cast<uintptr_t>(dy) & 15) && !(reinterpret_cast<uintptr_t>(x1) & 15) &&
+                   !(c2 && (reinterpret_cast<uintptr_t>(x2) & 15));
+  const WgradPlan pl = wgrad_plan(cout, cin, a.g, tma);
   if (pl.steps > 0x7FFFFFFFL) return fail("conv3_wgrad: too many rows");
   const long chunks = pl.chunks;
   a.kt = pl.kt;
@@ -1341,9 +1511,20 @@ int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, cons
   const int smem = pl.smem;
   if (smem > 227 * 1024) return fail("conv3_wgrad: stage too large");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  TRTT_CK(set_smem(k_conv3_wgrad, smem));
   dim3 grid(9, (unsigned)chunks);
-  k_conv3_wgrad<<<grid, 128, smem, st>>>(a);
+  if (tma) {
+    WgradMaps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    bool ok = act_map(&maps.dy, dy, cout, a.g.rows, 128) && act_map(&maps.x1, x1, c1, a.g.rows, 128) &&
+              act_map(&maps.x1_tail, x1, c1, a.g.rows, 2);
+    if (c2) ok = ok && act_map(&maps.x2, x2, c2, a.g.rows, 128) && act_map(&maps.x2_tail, x2, c2, a.g.rows, 2);
+    if (!ok) return fail("conv3_wgrad: tensor map encoding failed");
+    TRTT_CK(set_smem(k_conv3_wgrad_tma, smem));
+    k_conv3_wgrad_tma<<<grid, 128, smem, st>>>(a, maps);
+  } else {
+    TRTT_CK(set_smem(k_conv3_wgrad, smem));
+    k_conv3_wgrad<<<grid, 128, smem, st>>>(a);
+  }
   const long nw = (long)cout * 27 * cin;
   k_sum_parts<<<grid_for(nw), 256, 0, st>>>(a.part, (int)chunks, nw, dw);
   count_launch(2);
