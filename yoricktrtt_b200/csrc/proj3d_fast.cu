@@ -1,12 +1,17 @@
-// proj3d_fast.cu -- closed-form (cubic) 3D projector pair for column-
-// factorised views, two voxels per lane with packed FP32x2 arithmetic.
+// proj3d_fast.cu -- per-view 3D projector pair for column-factorised views
+// (circular orbits), both footprint models.
 //
-// Same decomposition as proj3d.cu (direct: detector-row bands in shared
-// memory; transpose: one warp per voxel column gathering through the
-// column's v-collapsed detector profile), but every lane handles voxel pairs
-// (k, k+32) so that the footprint scales and the B-spline primitive of both
-// voxels are evaluated by the same FFMA2/FMUL2/FADD2 instructions
-// (fast3d.cuh).
+// Direct: one CTA per (band of detector rows, view) accumulates the band in
+// shared memory; its warps pull 32-column chunks, build each hit column's
+// u-profile and spread it over the band rows with the column's v-weights
+// (fast3d_items.cuh: band_item for the closed-form cubic footprint, two
+// voxels per lane with packed FP32x2 arithmetic; band_item_table for the
+// tabulated footprint, with the reference's exact FP64 per-voxel axes).
+// Every detector cell has one owning CTA: no global atomics.  Transpose:
+// one warp per voxel column and k range gathers, view by view, through the
+// column's v-collapsed detector profile (column_item), Kahan-compensated,
+// atomic-free.  Both directions call the same footprint functions, so the
+// pair is an exact adjoint up to FP32 summation.
 #include <cuda_runtime.h>
 
 #include <climits>
