@@ -1346,6 +1346,7 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   // of the 128^3 U-Net: 1.18 / 1.37 / 1.73 ms)
   int tma = g_conv_tma < 0 ? (encode_tiled() ? 2 : 0) : g_conv_tma;
   if (tma == 2 && pow2_cols(2 * S * n) > 512) tma = 1;
+  if (a.g.rows < 256) tma = 0;  // tensors shorter than one 256-row box: cp.async
   // persistent tiles of 4 x 128 rows where two CTAs still fit on an SM
   // (tensor memory 2 x 4 n columns <= 256, and shared memory): the slab of a
   // tile overlaps the next tile's by 2 (w+2) + 2 rows, so longer tiles stage
@@ -1491,7 +1492,7 @@ int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, cons
   // staging: TMA unless cp.async is asked for (trtt_b200_conv3_set_tma(0)) or
   // the driver has no tensor-map encoder; rows must be addressable by the
   // 32-bit coordinates of a tensor copy, the tensors 16-byte aligned
-  const bool tma = g_conv_tma != 0 && encode_tiled() && a.g.rows + 512 < 0x7FFFFFFFL &&
+  const bool tma = g_conv_tma != 0 && encode_tiled() && a.g.rows >= 256 && a.g.rows + 512 < 0x7FFFFFFFL &&
                    !(reinterpret_cast<uintptr_t>(dy) & 15) && !(reinterpret_cast<uintptr_t>(x1) & 15) &&
                    !(c2 && (reinterpret_cast<uintptr_t>(x2) & 15));
   const WgradPlan pl = wgrad_plan(cout, cin, a.g, tma);
