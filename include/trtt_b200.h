@@ -549,7 +549,9 @@ size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, in
  * memory, tensor-memory columns, tiles.  which = 1: weight gradient,
  * info[0..9] = rows per stage, A and B chunk strides, A and B region bytes,
  * stages, dynamic shared memory, tensor-memory columns, row chunks, stages
- * per chunk. */
+ * per chunk.  which = 0 and 1 describe the cp.async staging; which = 2 the
+ * persistent TMA forward kernel (layout of 0), which = 3 the TMA weight
+ * gradient (layout of 1). */
 int trtt_b200_conv3_plan_info(int which, int cin, int cout, int nb, int d, int h, int w, long *info);
 int trtt_b200_conv3_wgrad(const void *dy, int cout, const void *x1, int c1, const void *x2, int c2,
                           float *dw, float *db, void *scratch, size_t scratch_bytes, int nb, int d,

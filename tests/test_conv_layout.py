@@ -218,3 +218,125 @@ def test_wgrad_emulation_reproduces_weight_gradient():
         ok = (p + o >= 0) & (p + o < g["rows"])
         ref[:, tap] = dY[p[ok]].T @ X[p[ok] + o]
     assert np.abs(dW - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cin,cout", NET_FWD)
+def test_forward_persistent_plan_bounds_at_128(cin, cout):
+    """The persistent TMA forward kernel's plan (tiles of 4 x 128 rows where
+    two CTAs still fit on an SM, else 2 x 128): every TMA box (8 channels x
+    256 rows, and the tail box) lands 128-byte aligned inside its chunk, the
+    stage's transaction bytes fit the stage, the taps' A reads stay in the
+    slab, and the two tensor-memory accumulators fit the CTAs per SM."""
+    for n in (128, 64, 32):
+        S, rh, cs, stage, nstg, smem, tmem_cols, tiles = _plan(2, cin, cout, 1, n, n, n)[:8]
+        g = _grid(1, n, n, n)
+        assert S in (2, 4) and (S == 2 or cout <= 32)
+        if n == 128 and cout <= 32:
+            assert S == 4  # the 16- and 32-channel layers at full size
+        assert smem <= SMEM_MAX and nstg * stage <= smem
+        assert 2 * S * cout <= tmem_cols <= 512
+        if S == 4:
+            assert 2 * (smem + 2048) <= SMEM_MAX and 2 * tmem_cols <= 512
+        assert rh == 128 * S + 2 * g["wp"] + 2 and cs % 128 == 0 and stage % 1024 == 0
+        boxes = [(r0, min(256, rh - r0)) for r0 in range(0, rh, 256)]
+        assert sum(b for _, b in boxes) == rh
+        for c in range(2):
+            for r0, b in boxes:
+                dst = c * cs + r0 * 16
+                assert dst % 128 == 0 and r0 * 16 + b * 16 <= cs
+        assert 2 * rh * 16 + 288 * cout <= stage  # the stage's transaction bytes
+        a_end = _kmajor((2 * g["wp"] + 2 + 128 * (S - 1)) * 16, cs, 128, 128).max() + 2
+        assert a_end <= 2 * cs
+        assert tiles * 128 * S >= g["rows"] - 2 * g["plane"]
+
+
+@pytest.mark.parametrize("cout,cin", NET_WGRAD)
+def test_wgrad_tma_plan_bounds_at_128(cout, cin):
+    """The TMA weight gradient's plan: chunk strides of whole 128-byte
+    lines, every box (8 channels x 128 rows, the 2-row tail of the input
+    halo) 128-byte aligned inside its chunk and region, and the MMAs' reads
+    inside the allocation."""
+    for n in (128, 64, 32):
+        kt, csa, csb, ab, bb, nstg, smem, tmem_cols, chunks, steps = _plan(3, cin, cout, 1, n, n, n)
+        g = _grid(1, n, n, n)
+        nca, ncb = cout // 8, cin // 8
+        assert smem <= SMEM_MAX and tmem_cols >= 3 * cin and kt % 128 == 0
+        assert csa % 128 == 0 and csb % 128 == 0 and ab % 128 == 0 and bb % 128 == 0
+        for buf in range(nstg):
+            a0, b0 = buf * ab, nstg * ab + buf * bb
+            for c in range(nca):
+                for r0 in range(0, kt, 128):
+                    dst = a0 + c * csa + r0 * 16
+                    assert dst % 128 == 0 and r0 * 16 + 128 * 16 <= csa and dst + 2048 <= a0 + ab
+            for c in range(ncb):
+                for r0 in range(0, kt, 128):
+                    dst = b0 + c * csb + r0 * 16
+                    assert dst % 128 == 0 and dst + 2048 <= b0 + bb
+                tail = b0 + c * csb + kt * 16
+                assert tail % 128 == 0 and kt * 16 + 2 * 16 <= csb and tail + 32 <= b0 + bb
+            ks = kt // 16 - 1
+            assert _mnmajor(a0 + ks * 256, 128, csa, 64).max() + 2 <= smem
+            assert _mnmajor(b0 + (ks * 16 + 2) * 16, 128, csb, cin).max() + 2 <= smem
+        total = -(-(g["rows"] - 2 * g["plane"]) // kt)
+        assert chunks * steps >= total and (chunks - 1) * steps < total
+
+
+def test_wgrad_tma_emulation_reproduces_weight_gradient():
+    """The TMA staging loads whole boxes: dY rows at or past the end of the
+    summed range are the last z border plane (zero by the layout) or lie
+    past the tensor (read as zero), and input rows before the first row
+    read as zero.  With the TMA plan's layout and those reads the MMAs
+    reproduce the weight gradient."""
+    rng = np.random.default_rng(2)
+    nb, d, h, w, cout, c1, c2 = 2, 3, 4, 5, 16, 16, 16
+    cin = c1 + c2
+    kt, csa, csb, ab, bb, nstg, smem, tmem_cols, chunks, steps = _plan(3, cin, cout, nb, d, h, w)
+    g = _grid(nb, d, h, w)
+    dY = _padded(rng, nb, d, h, w, cout)
+    X = np.concatenate([_padded(rng, nb, d, h, w, c1), _padded(rng, nb, d, h, w, c2)], 1)
+    nca, ncb = cout // 8, cin // 8
+    r0, r1 = g["plane"], g["rows"] - g["plane"]
+
+    def box(sm, dst, T, x, y, rows):
+        for r in range(rows):
+            row = y + r
+            ok = 0 <= row < g["rows"]
+            sm.cp16(dst + r * 16, T[row, x:x + 8] if ok else np.zeros(8))
+
+    dW = np.zeros((cout, 27, cin))
+    for gidx in range(9):
+        dzi, dyi = divmod(gidx, 3)
+        off = (dzi - 1) * g["plane"] + (dyi - 1) * g["wp"]
+        for cy in range(chunks):
+            qbeg = r0 + cy * steps * kt
+            T = 0 if r1 - qbeg <= 0 else min(steps, -(-(r1 - qbeg) // kt))
+            acc = np.zeros((3, 64, cin))
+            sm = Smem(smem)
+            sm.v[:] = 0.0  # rows above cout read whatever lies there; not read back
+            for it in range(T):
+                buf = it % nstg
+                a0, b0 = buf * ab, nstg * ab + buf * bb
+                q0 = qbeg + it * kt
+                hb = q0 + off - 1
+                for c in range(nca):
+                    for rr in range(0, kt, 128):
+                        box(sm, a0 + c * csa + rr * 16, dY, 8 * c, q0 + rr, 128)
+                for c in range(ncb):
+                    for rr in range(0, kt, 128):
+                        box(sm, b0 + c * csb + rr * 16, X, 8 * c, hb + rr, 128)
+                    box(sm, b0 + c * csb + kt * 16, X, 8 * c, hb + kt, 2)
+                for ks in range(kt // 16):
+                    A = sm.read(_mnmajor(a0 + ks * 256, 128, csa, 64))
+                    for j in range(3):
+                        B = sm.read(_mnmajor(b0 + (ks * 16 + j) * 16, 128, csb, cin))
+                        acc[j] += A @ B.T
+            for j in range(3):
+                dW[:, gidx * 3 + j] += acc[j, :cout]
+    ref = np.zeros((cout, 27, cin))
+    for tap in range(27):
+        dz, dy, dx = tap // 9 - 1, (tap // 3) % 3 - 1, tap % 3 - 1
+        o = dz * g["plane"] + dy * g["wp"] + dx
+        p = np.arange(r0, r1)
+        ok = (p + o >= 0) & (p + o < g["rows"])
+        ref[:, tap] = dY[p[ok]].T @ X[p[ok] + o]
+    assert np.abs(dW - ref).max() <= 1e-12 * np.abs(ref).max()

@@ -1214,6 +1214,26 @@ FwdPlan fwd_plan_tma(int n, int groups, const Grid3 &g, int S = kFwdS)
   return p;
 }
 
+// Stage layout of the persistent TMA forward kernel: tiles of 4 x 128 rows
+// where two CTAs still fit on an SM (tensor memory 2 x 4 n columns <= 256,
+// and shared memory), else 2 x 128; two tensor-memory accumulators.  *S
+// receives the sub-tiles per tile.
+FwdPlan fwd_plan_pers(int n, int groups, const Grid3 &g, int *S)
+{
+  int s = kFwdS;
+  if (pow2_cols(2 * 4 * n) <= 256) {
+    FwdPlan p4 = fwd_plan_tma(n, groups, g, 4);
+    p4.nstg = 4 * p4.stage_bytes <= 112 * 1024 ? 4 : 3;
+    if (2 * ((long)residency_smem(p4.nstg * p4.stage_bytes, pow2_cols(2 * 4 * n)) + 2048) <= 227L * 1024) s = 4;
+  }
+  FwdPlan p = fwd_plan_tma(n, groups, g, s);
+  p.tmem_cols = pow2_cols(2 * s * n);
+  p.nstg = 4 * p.stage_bytes <= 112 * 1024 ? 4 : 3;
+  p.smem = residency_smem(p.nstg * p.stage_bytes, p.tmem_cols);
+  *S = s;
+  return p;
+}
+
 // cuTensorMapEncodeTiled, reached through the runtime (no driver library
 // link); null when the driver does not provide it.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -1343,28 +1363,19 @@ int trtt_b200_conv3_forward(const void *x1, int c1, const void *x2, int c2, cons
   // staging: 0 cp.async, 1 TMA per tile, 2 TMA persistent (two tensor-memory
   // accumulators: 2 S n columns must fit in 512); automatic: the persistent
   // kernel where it applies, else TMA per tile, else cp.async (forward pass
-  // of the 128^3 U-Net: 1.18 / 1.37 / 1.73 ms)
+  // of the 128^3 U-Net: 1.03 / 1.37 / 1.73 ms)
   int tma = g_conv_tma < 0 ? (encode_tiled() ? 2 : 0) : g_conv_tma;
   if (tma == 2 && pow2_cols(2 * S * n) > 512) tma = 1;
   if (a.g.rows < 256) tma = 0;  // tensors shorter than one 256-row box: cp.async
-  // persistent tiles of 4 x 128 rows where two CTAs still fit on an SM
-  // (tensor memory 2 x 4 n columns <= 256, and shared memory): the slab of a
-  // tile overlaps the next tile's by 2 (w+2) + 2 rows, so longer tiles stage
-  // each input row fewer times (1.5 instead of 2 slab rows per output row
-  // at 128^3) and fetch each stage's weights for twice the rows
-  bool s4 = false;
-  if (tma == 2 && pow2_cols(2 * 4 * n) <= 256) {
-    FwdPlan p4 = fwd_plan_tma(n, a.groups, a.g, 4);
-    p4.nstg = 4 * p4.stage_bytes <= 112 * 1024 ? 4 : 3;
-    s4 = 2 * ((long)residency_smem(p4.nstg * p4.stage_bytes, pow2_cols(2 * 4 * n)) + 2048) <= 227L * 1024;
-  }
+  // persistent kernel: tiles of 4 x 128 rows where two CTAs still fit on an
+  // SM (fwd_plan_pers).  The slab of a tile overlaps the next tile's by
+  // 2 (w+2) + 2 rows, so longer tiles stage each input row fewer times (1.5
+  // instead of 2 slab rows per output row at 128^3) and fetch each stage's
+  // weights for twice the rows (forward pass 1.18 -> 1.03 ms)
+  int sp = S;
   if (tma) {
-    FwdPlan pl = fwd_plan_tma(n, a.groups, a.g, s4 ? 4 : S);
-    if (tma == 2) {
-      pl.tmem_cols = pow2_cols(2 * (s4 ? 4 : S) * n);
-      pl.nstg = 4 * pl.stage_bytes <= 112 * 1024 ? 4 : 3;
-      pl.smem = residency_smem(pl.nstg * pl.stage_bytes, pl.tmem_cols);
-    }
+    const FwdPlan pl = tma == 2 ? fwd_plan_pers(n, a.groups, a.g, &sp) : fwd_plan_tma(n, a.groups, a.g);
+    const bool s4 = sp == 4;
     a.rh = pl.rh;
     a.cs = pl.cs;
     a.stage_bytes = pl.stage_bytes;
@@ -1451,13 +1462,21 @@ int trtt_b200_conv3_plan_info(int which, int cin, int cout, int nb, int d, int h
     for (int i = 0; i < 8; ++i) info[i] = v[i];
     return 0;
   }
-  if (which == 1) {
-    const WgradPlan p = wgrad_plan(cout, cin, g);
+  if (which == 1 || which == 3) {
+    const WgradPlan p = wgrad_plan(cout, cin, g, which == 3);
     const long v[] = {p.kt, p.csa, p.csb, p.a_bytes, p.b_bytes, p.nstg, p.smem, p.tmem_cols, p.chunks, p.steps};
     for (int i = 0; i < 10; ++i) info[i] = v[i];
     return 0;
   }
-  return fail("conv3_plan_info: which must be 0 (forward) or 1 (weight gradient)");
+  if (which == 2) {
+    int S = kFwdS;
+    const FwdPlan p = fwd_plan_pers(cout, cin / 16, g, &S);
+    const long v[] = {S, p.rh, p.cs, p.stage_bytes, p.nstg, p.smem, p.tmem_cols, p.tiles};
+    for (int i = 0; i < 8; ++i) info[i] = v[i];
+    return 0;
+  }
+  return fail("conv3_plan_info: which must be 0 (forward, cp.async), 1 (weight gradient, cp.async), "
+              "2 (forward, persistent TMA) or 3 (weight gradient, TMA)");
 }
 
 size_t trtt_b200_conv3_wgrad_scratch(int cout, int cin, int nb, int d, int h, int w)
