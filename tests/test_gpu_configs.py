@@ -194,6 +194,57 @@ def test_c3_table_slot_flips(oracle_port, c3):
     assert flips == 0
 
 
+def test_c3_batch_call_host_buffers(oracle_port, c3):
+    """The end-to-end path at the benchmarked size: trtt_b200_cb3d_batch_ex
+    on pinned host FP64 arrays in the reference layouts, as the bench's e2e
+    leg calls it (view groups; direct view chunks alternating over two
+    streams with each chunk's read-back overlapping later chunks; the
+    transpose's upload chunks growing by half).  Overwrite mode (out = H in)
+    on sampled views of the forward and on the transpose of a stack that is
+    random on the sampled views, against the FP64 oracle; then the plugin's
+    accumulate mode (out += H in) on top of the forward result."""
+    import torch
+    from yoricktrtt_b200 import _lib
+    lib = _lib.load()
+    sc, vol = c3
+    vol64 = torch.from_numpy(np.ascontiguousarray(vol, dtype=np.float64)).pin_memory().numpy()
+    det = torch.full((sc.nviews, sc.nv, sc.nu), 7.0, dtype=torch.float64).pin_memory().numpy()
+    xos, xsd = np.ascontiguousarray(sc.xos), np.ascontiguousarray(sc.xsd)
+
+    def call(out, inp, job, accumulate):
+        rc = lib.trtt_b200_cb3d_batch_ex(_lib.dptr(out), _lib.dptr(inp), sc.nx, sc.ny, sc.nz, sc.s_scl,
+                                         sc.s_deg, None, 0, 1.0, None, sc.nu, sc.nv, sc.u_scl, sc.v_scl,
+                                         sc.nviews, _lib.dptr(xos), _lib.dptr(xsd), G.TRTT_CONE_BEAM, job,
+                                         accumulate)
+        _lib.check(rc, "trtt_b200_cb3d_batch_ex")
+
+    call(det, vol64, 0, 0)
+    got = {v: det[v].copy() for v in C3_SAMPLE}
+    worst, errs = _check_forward(oracle_port, sc, vol, got)
+    print(f"C3 batch call forward rel-L2 per view: {['%.2e' % e for e in errs]}")
+    assert worst <= TOL
+    call(det, vol64, 0, 1)  # accumulate: twice the projection
+    assert max(rel_l2(det[v], 2.0 * got[v]) for v in C3_SAMPLE[:3]) <= 1e-6
+    rng = np.random.default_rng(4)
+    y = torch.zeros((sc.nviews, sc.nv, sc.nu), dtype=torch.float64).pin_memory().numpy()
+    for v in C3_SAMPLE:
+        y[v] = rng.random((sc.nv, sc.nu))
+    back = torch.full((sc.nz, sc.ny, sc.nx), 3.0, dtype=torch.float64).pin_memory().numpy()
+    call(back, y, 1, 0)
+
+    def ref(v):
+        out = np.zeros((sc.nz, sc.ny, sc.nx))
+        assert oracle_port._p3d("CB3D", out, np.ascontiguousarray(y[v]), sc, v, 1, None) == 0
+        return out
+
+    total = np.zeros_like(back)
+    for r in _pmap(ref, C3_SAMPLE):
+        total += r
+    err_b = rel_l2(back, total)
+    print(f"C3 batch call transpose rel-L2: {err_b:.2e}")
+    assert err_b <= TOL
+
+
 # ---------------------------------------------------------------------------
 # 2D fan beam 512^2 -> 720 x 1024
 # ---------------------------------------------------------------------------
