@@ -346,8 +346,11 @@ def run_dropin_e2e(sc, vol_h, nsample=8):
             "path": "trtt_CB3D_cubic per view and direction (the symbol the Yorick closure "
                     "_trtt_single_3D_projector calls), pageable host FP64 arrays, out += H in",
             "sample": f"{nsample} view pairs of the workload, per-pair time scaled to the rate",
-            "h2d_bytes_per_view_pair": 8 * (nvox + npix) + 8 * (npix + nvox),
-            "d2h_bytes_per_view_pair": 8 * npix + 8 * nvox}
+            # direct: the FP64 volume up, the image (accumulated) up and
+            # down; transpose: the FP64 image up, the volume's FP32
+            # contribution down (added into the host volume on the host)
+            "h2d_bytes_per_view_pair": 8 * (nvox + npix) + 8 * npix,
+            "d2h_bytes_per_view_pair": 8 * npix + 4 * nvox}
 
 
 def run_b200(args):

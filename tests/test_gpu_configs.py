@@ -245,6 +245,35 @@ def test_c3_batch_call_host_buffers(oracle_port, c3):
     assert err_b <= TOL
 
 
+def test_c3_dropin_per_view_pageable(oracle_port, c3):
+    """The symbol an unchanged Yorick closure calls, trtt_CB3D_cubic, one
+    view per call on pageable FP64 arrays at the benchmarked size: the
+    volume upload passes through the pinned staging ring in several slots,
+    and the transpose adds its FP32 result into the host volume on the host
+    (two slots).  out += H in (and H^T) on pre-filled outputs, against the
+    FP64 oracle."""
+    from yoricktrtt_b200 import dropin
+    sc, vol = c3
+    vol64 = np.ascontiguousarray(vol, dtype=np.float64)
+    rng = np.random.default_rng(6)
+    for v in (0, 137):
+        pre = rng.random((sc.nv, sc.nu))
+        got = pre.copy()
+        ref = pre.copy()
+        dropin.scan3d_call("CB3D", got, vol64, sc, v, 0, None)
+        assert oracle_port._p3d("CB3D", ref, vol64, sc, v, 0, None) == 0
+        assert rel_l2(got - pre, ref - pre) <= TOL
+        y = rng.random((sc.nv, sc.nu))
+        pre_b = rng.random((sc.nz, sc.ny, sc.nx))
+        got_b = pre_b.copy()
+        ref_b = pre_b.copy()
+        dropin.scan3d_call("CB3D", got_b, y, sc, v, 1, None)
+        assert oracle_port._p3d("CB3D", ref_b, y, sc, v, 1, None) == 0
+        err = rel_l2(got_b - pre_b, ref_b - pre_b)
+        print(f"C3 per-view drop-in view {v}: forward {rel_l2(got - pre, ref - pre):.2e}, transpose {err:.2e}")
+        assert err <= TOL
+
+
 # ---------------------------------------------------------------------------
 # 2D fan beam 512^2 -> 720 x 1024
 # ---------------------------------------------------------------------------

@@ -664,7 +664,7 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
     if (in_early)  // started on the copy stream before the grouping
       TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvIn], 0));
     else
-      TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nvox, cudaMemcpyHostToDevice, st));
+      TRTT_CK(upload_host(D, D.in64.p, in, sizeof(double) * nvox, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
@@ -743,8 +743,7 @@ int host3d_grouped(DropIn &D, const Params3D &P, double *out, const double *in,
       member_runs(lists[q], G, cb[c], cb[c + 1], runs);
       for (const auto &r : runs) {
         const long off = r.first * nview_px, cnt = (r.second - r.first) * nview_px;
-        TRTT_CK(cudaMemcpyAsync(D.in64.as<double>() + off, in + off, sizeof(double) * cnt,
-                                cudaMemcpyHostToDevice, cp));
+        TRTT_CK(upload_host(D, D.in64.as<double>() + off, in + off, sizeof(double) * cnt, cp));
         TRTT_CK(f64_to_f32(D.in64.as<double>() + off, D.det32.as<float>() + off, cnt, cp));
         count_launch();
       }
@@ -820,7 +819,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   // its upload overlaps the view grouping and the source-plane check below
   const bool in_early = job == 0 && fact && !cum;
   if (in_early) {
-    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, cp));
+    TRTT_CK(upload_host(D, D.in64.p, in, sizeof(double) * nin, cp));
     TRTT_CK(cudaEventRecord(D.ev[DropIn::kEvIn], cp));
   }
   std::vector<int> glists[3];
@@ -829,6 +828,11 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     find_view_groups(nx, ny, nviews, xos, xsd, glists);
     grouped = !glists[1].empty() || !glists[2].empty();
   }
+  // the transpose of per-view calls (the plugin's accumulate into a
+  // pageable host volume, as a Yorick closure makes them): the result is
+  // added into `out` on the host (download_add) instead of uploading `out`
+  const bool host_add = job == 1 && accumulate && !grouped && sizeof(double) * nout >= (4u << 20) &&
+                        !host_pinned(out);
   if (grouped && job == 0) {
     // the source-plane pre-check of the per-view path below, then the group
     // kernels
@@ -866,7 +870,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     if (in_early)
       TRTT_CK(cudaStreamWaitEvent(st, D.ev[DropIn::kEvIn], 0));
     else
-      TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+      TRTT_CK(upload_host(D, D.in64.p, in, sizeof(double) * nin, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
     TRTT_CK(cudaMemsetAsync(D.det32.p, 0, sizeof(float) * npix, st));
@@ -911,7 +915,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     TRTT_CK(cudaStreamSynchronize(st));
     return 0;
   } else if (job == 0) {
-    TRTT_CK(cudaMemcpyAsync(D.in64.p, in, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+    TRTT_CK(upload_host(D, D.in64.p, in, sizeof(double) * nin, st));
     TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
     TRTT_CK(xyz_f64_to_col_f32(D.in64.as<double>(), D.vol32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
@@ -960,7 +964,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     for (size_t c = 0; c + 1 < cb.size(); ++c) {
       const long v0 = cb[c], v1 = cb[c + 1];
       const long off = v0 * nu * nv, cnt = (v1 - v0) * nu * nv;
-      TRTT_CK(cudaMemcpyAsync(D.in64.as<double>() + off, in + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, cp));
+      TRTT_CK(upload_host(D, D.in64.as<double>() + off, in + off, sizeof(double) * cnt, cp));
       TRTT_CK(f64_to_f32(D.in64.as<double>() + off, D.det32.as<float>() + off, cnt, cp));
       TRTT_CK(cudaEventRecord(D.ev[2 + c], cp));
       TRTT_CK(cudaStreamWaitEvent(st, D.ev[2 + c], 0));
@@ -970,7 +974,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
       TRTT_CK(launch_back3d(L, st));
       count_launch(2);
     }
-    TRTT_CK(out_to_device(cp));
+    if (!host_add) TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
   }
   TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
@@ -980,6 +984,17 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   if (herr & TRTT_ERR_SOURCE_PLANE) {
     std::fprintf(stderr, "trtt_b200: a voxel lies in the source plane (wk == 0); out left unchanged\n");
     return fail("a voxel lies in the source plane (wk == 0)");
+  }
+  if (host_add) {
+    // out += result on the host: the volume comes back in FP32 (half the
+    // bytes of the FP64 round trip, and no upload of `out`) through the
+    // pinned staging ring, and host threads make the same FP64 additions
+    TRTT_CK(D.xyz32.ensure(sizeof(float) * nvox));
+    TRTT_CK(cudaMemsetAsync(D.xyz32.p, 0, sizeof(float) * nvox, st));
+    TRTT_CK(col_f32_add_to_xyz_f32(D.vol32.as<float>(), D.xyz32.as<float>(), (int)nx, (int)ny, (int)nz, 1, st));
+    count_launch();
+    TRTT_CK(download_add(D, out, D.xyz32.as<float>(), nvox, st));
+    return 0;
   }
   // out += result (FP64 accumulation on the device; out64 holds out already)
   if (job == 0) {

@@ -2,9 +2,13 @@
 // libtrtt_b200.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "runtime.h"
 
@@ -90,6 +94,110 @@ cudaError_t DropIn::init()
     if (e != cudaSuccess) return e;
   }
   ready = true;
+  return cudaSuccess;
+}
+
+cudaError_t DropIn::init_stage()
+{
+  for (int i = 0; i < 2; ++i) {
+    if (stage[i]) continue;
+    cudaError_t e = cudaHostAlloc(&stage[i], kStageBytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) return e;
+    e = cudaEventCreateWithFlags(&stage_ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+bool host_pinned(const void *p)
+{
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
+namespace {
+
+// fn(lo, hi) over [0, n) split among up to 16 host threads (one slice each).
+template <typename F>
+void host_parallel(long n, F fn)
+{
+  const long min_slice = 1L << 18;
+  unsigned hw = std::thread::hardware_concurrency();
+  long nt = std::min<long>(hw ? hw : 1, 16);
+  nt = std::max<long>(1, std::min<long>(nt, n / min_slice));
+  if (nt <= 1) {
+    fn(0L, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  const long per = (n + nt - 1) / nt;
+  for (long t = 1; t < nt; ++t) {
+    const long lo = t * per, hi = std::min(n, lo + per);
+    if (lo < hi) th.emplace_back(fn, lo, hi);
+  }
+  fn(0L, std::min(n, per));
+  for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+cudaError_t upload_host(DropIn &D, void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+  if (bytes < (4u << 20) || host_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e = D.init_stage();
+  if (e != cudaSuccess) return e;
+  const char *sp = static_cast<const char *>(src);
+  char *dp = static_cast<char *>(dst);
+  int k = 0;
+  for (size_t off = 0; off < bytes; off += DropIn::kStageBytes, ++k) {
+    const int slot = k & 1;
+    const size_t len = std::min(DropIn::kStageBytes, bytes - off);
+    e = cudaEventSynchronize(D.stage_ev[slot]);  // the slot's previous copy has left it
+    if (e != cudaSuccess) return e;
+    char *stg = static_cast<char *>(D.stage[slot]);
+    host_parallel((long)len, [&](long lo, long hi) { std::memcpy(stg + lo, sp + off + lo, (size_t)(hi - lo)); });
+    e = cudaMemcpyAsync(dp + off, stg, len, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(D.stage_ev[slot], s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t download_add(DropIn &D, double *out, const float *src, long n, cudaStream_t s)
+{
+  cudaError_t e = D.init_stage();
+  if (e != cudaSuccess) return e;
+  const long chunk = (long)(DropIn::kStageBytes / sizeof(float));
+  const long nchunks = (n + chunk - 1) / chunk;
+  auto issue = [&](long k) -> cudaError_t {
+    const int slot = (int)(k & 1);
+    const long lo = k * chunk, len = std::min(chunk, n - lo);
+    cudaError_t r = cudaEventSynchronize(D.stage_ev[slot]);  // no upload still reads the slot
+    if (r != cudaSuccess) return r;
+    r = cudaMemcpyAsync(D.stage[slot], src + lo, sizeof(float) * len, cudaMemcpyDeviceToHost, s);
+    if (r != cudaSuccess) return r;
+    return cudaEventRecord(D.stage_ev[slot], s);
+  };
+  if (nchunks > 0 && (e = issue(0)) != cudaSuccess) return e;
+  for (long k = 0; k < nchunks; ++k) {
+    // slot (k+1) & 1 held chunk k-1, whose additions are done
+    if (k + 1 < nchunks && (e = issue(k + 1)) != cudaSuccess) return e;
+    const int slot = (int)(k & 1);
+    e = cudaEventSynchronize(D.stage_ev[slot]);
+    if (e != cudaSuccess) return e;
+    const float *stg = static_cast<const float *>(D.stage[slot]);
+    double *o = out + k * chunk;
+    const long len = std::min(chunk, n - k * chunk);
+    host_parallel(len, [&](long lo, long hi) {
+      for (long i = lo; i < hi; ++i) o[i] += (double)stg[i];
+    });
+  }
   return cudaSuccess;
 }
 

@@ -47,10 +47,33 @@ struct DropIn {
   static constexpr int kEvIn = kChunks + 2;
   static constexpr int kEvents = kChunks + 5;
   cudaEvent_t ev[kEvents] = {};
-  DevBuf in64, out64, vol32, det32, geom, gates, aux, err, grp;
+  DevBuf in64, out64, vol32, det32, geom, gates, aux, err, grp, xyz32;
+  // Pinned staging ring for pageable host arrays (the arrays of a Yorick
+  // caller): two slots of kStageBytes, each with the event of its last copy.
+  static constexpr size_t kStageBytes = 32u << 20;
+  void *stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {};
   cudaError_t init();
+  cudaError_t init_stage();
 };
 DropIn &dropin();
+
+// True when host memory at p is registered with (or allocated by) CUDA:
+// copies from it run at full DMA speed and asynchronously.
+bool host_pinned(const void *p);
+
+// dst (device) <- src (host) on stream s.  From pinned memory one
+// asynchronous copy; from pageable memory of at least 4 MB the bytes pass
+// through D's pinned staging ring (host threads fill a slot while the
+// previous slot's DMA runs).  Returns when src may be reused; the copies may
+// still be in flight on s.
+cudaError_t upload_host(DropIn &D, void *dst, const void *src, size_t bytes, cudaStream_t s);
+
+// out[i] += (double)src[i] for i < n (src on the device, out pageable host
+// memory): the FP32 values come back through the pinned staging ring and
+// host threads add each slot while the next slot's DMA runs.  The same
+// FP64 additions as on the device.  Synchronous.
+cudaError_t download_add(DropIn &D, double *out, const float *src, long n, cudaStream_t s);
 
 // Report a CUDA error and return -1 (for use in `return fail_cuda(...)`).
 int fail_cuda(cudaError_t e, const char *what);
