@@ -177,6 +177,46 @@ def test_group_batch_entry_point(oracle_port, case, job):
     assert rel_l2(out, 2 * ref) <= TOL
 
 
+@pytest.mark.parametrize("job", [0, 1])
+def test_group_batch_pageable_large(oracle_port, job):
+    """The batch call on pageable (numpy) arrays of more than 4 MB: the
+    input passes through the pinned staging ring, and the accumulated
+    transpose is added into the host volume on the host (the FP32
+    contribution comes back, not an FP64 round trip of out); overwrite and
+    accumulate modes, grouped views."""
+    from yoricktrtt_b200 import _lib
+    sc = _scan(nx=96, ny=96, nz=96, nu=128, nv=128, views=8, rsc=300.0, rsd=450.0)
+    rng = np.random.default_rng(17)
+    vol = np.ascontiguousarray(P.ellipsoids_3d(sc.nx, sc.ny, sc.nz, n=6, seed=5, dtype=np.float64))
+    det = rng.random((sc.nviews, sc.nv, sc.nu))
+    inp = vol if job == 0 else det
+    shape = (sc.nviews, sc.nv, sc.nu) if job == 0 else vol.shape
+    assert 8 * vol.size >= 4 << 20  # the volume passes the 4 MB staging threshold
+    ref = np.zeros(shape)
+    for v in range(sc.nviews):
+        if job == 0:
+            oracle_port.cb3d(ref[v], vol, sc, v, 0)
+        else:
+            oracle_port.cb3d(ref, np.ascontiguousarray(det[v]), sc, v, 1)
+    lib = _lib.load()
+    xos, xsd = np.ascontiguousarray(sc.xos), np.ascontiguousarray(sc.xsd)
+
+    def call(out, acc):
+        rc = lib.trtt_b200_cb3d_batch_ex(
+            _lib.dptr(out), _lib.dptr(inp), sc.nx, sc.ny, sc.nz, sc.s_scl, sc.s_deg, None, 0,
+            1.0, None, sc.nu, sc.nv, sc.u_scl, sc.v_scl, sc.nviews, _lib.dptr(xos),
+            _lib.dptr(xsd), 4, job, acc)
+        assert rc == 0, _lib.last_error()
+
+    out = np.full(shape, np.nan)
+    call(out, 0)
+    assert np.isfinite(out).all() and rel_l2(out, ref) <= TOL
+    pre = rng.random(shape)
+    out = pre.copy()
+    call(out, 1)
+    assert rel_l2(out - pre, ref) <= TOL
+
+
 def test_group_quad_shapes(oracle_port):
     """Other shapes of the quad direct kernel (band rows, cells per u tile,
     CTAs per SM with their register budget) give the same projection."""

@@ -811,7 +811,12 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   // read-back of out64 is done.
   TRTT_CK(cudaEventRecord(D.ev[0], st));
   TRTT_CK(cudaStreamWaitEvent(cp, D.ev[0], 0));
+  // a transpose accumulated into a pageable host volume (a Yorick caller's
+  // array) is added into `out` on the host at the end (download_add)
+  // instead of taking `out` to the device and back
+  const bool host_add = job == 1 && accumulate && sizeof(double) * nout >= (4u << 20) && !host_pinned(out);
   auto out_to_device = [&](cudaStream_t s) -> cudaError_t {
+    if (host_add) return cudaSuccess;
     if (accumulate) return cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);
     return cudaMemsetAsync(D.out64.p, 0, sizeof(double) * nout, s);
   };
@@ -828,11 +833,6 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
     find_view_groups(nx, ny, nviews, xos, xsd, glists);
     grouped = !glists[1].empty() || !glists[2].empty();
   }
-  // the transpose of per-view calls (the plugin's accumulate into a
-  // pageable host volume, as a Yorick closure makes them): the result is
-  // added into `out` on the host (download_add) instead of uploading `out`
-  const bool host_add = job == 1 && accumulate && !grouped && sizeof(double) * nout >= (4u << 20) &&
-                        !host_pinned(out);
   if (grouped && job == 0) {
     // the source-plane pre-check of the per-view path below, then the group
     // kernels
@@ -974,7 +974,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
       TRTT_CK(launch_back3d(L, st));
       count_launch(2);
     }
-    if (!host_add) TRTT_CK(out_to_device(cp));
+    TRTT_CK(out_to_device(cp));
     TRTT_CK(cudaEventRecord(D.ev[1], cp));
   }
   TRTT_CK(cudaStreamWaitEvent(st, D.ev[1], 0));
