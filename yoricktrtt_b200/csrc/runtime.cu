@@ -138,7 +138,12 @@ void host_parallel(long n, F fn)
   const long per = (n + nt - 1) / nt;
   for (long t = 1; t < nt; ++t) {
     const long lo = t * per, hi = std::min(n, lo + per);
-    if (lo < hi) th.emplace_back(fn, lo, hi);
+    if (lo >= hi) continue;
+    try {
+      th.emplace_back(fn, lo, hi);
+    } catch (...) {
+      fn(lo, hi);  // no thread to be had: this slice on the calling thread
+    }
   }
   fn(0L, std::min(n, per));
   for (auto &x : th) x.join();
