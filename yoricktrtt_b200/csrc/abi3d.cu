@@ -814,7 +814,7 @@ int host3d(int geom, double *out, const double *in, long nx, long ny, long nz,
   // a transpose accumulated into a pageable host volume (a Yorick caller's
   // array) is added into `out` on the host at the end (download_add)
   // instead of taking `out` to the device and back
-  const bool host_add = job == 1 && accumulate && sizeof(double) * nout >= (4u << 20) && !host_pinned(out);
+  const bool host_add = job == 1 && accumulate && sizeof(double) * nout >= (4u << 20) && host_pageable(out);
   auto out_to_device = [&](cudaStream_t s) -> cudaError_t {
     if (host_add) return cudaSuccess;
     if (accumulate) return cudaMemcpyAsync(D.out64.p, out, sizeof(double) * nout, cudaMemcpyHostToDevice, s);

@@ -109,14 +109,14 @@ cudaError_t DropIn::init_stage()
   return cudaSuccess;
 }
 
-bool host_pinned(const void *p)
+bool host_pageable(const void *p)
 {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();  // clear the sticky-free error of an unknown pointer
-    return false;
+    cudaGetLastError();  // clear the non-sticky error of an unknown pointer
+    return true;
   }
-  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeUnregistered;
 }
 
 namespace {
@@ -153,7 +153,7 @@ void host_parallel(long n, F fn)
 
 cudaError_t upload_host(DropIn &D, void *dst, const void *src, size_t bytes, cudaStream_t s)
 {
-  if (bytes < (4u << 20) || host_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  if (bytes < (4u << 20) || !host_pageable(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
   cudaError_t e = D.init_stage();
   if (e != cudaSuccess) return e;
   const char *sp = static_cast<const char *>(src);

@@ -58,12 +58,13 @@ struct DropIn {
 };
 DropIn &dropin();
 
-// True when host memory at p is registered with (or allocated by) CUDA:
-// copies from it run at full DMA speed and asynchronously.
-bool host_pinned(const void *p);
+// True when p is ordinary pageable host memory (not allocated or registered
+// by CUDA, not device memory): copies from it are staged by the driver at a
+// fraction of the DMA speed.
+bool host_pageable(const void *p);
 
-// dst (device) <- src (host) on stream s.  From pinned memory one
-// asynchronous copy; from pageable memory of at least 4 MB the bytes pass
+// dst (device) <- src (host) on stream s.  From pinned (or device) memory
+// one asynchronous copy; from pageable memory of at least 4 MB the bytes pass
 // through D's pinned staging ring (host threads fill a slot while the
 // previous slot's DMA runs).  Returns when src may be reused; the copies may
 // still be in flight on s.
